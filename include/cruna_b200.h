@@ -1,0 +1,220 @@
+/*
+ * cruna_b200.h -- C ABI of the B200 (sm_100a) implementation of CRUNA's direct and adjoint
+ * compressible Navier-Stokes time step.
+ *
+ * Every entry point replaces one Fortran module procedure of CRUNA (cruna-toolkit/public); the
+ * procedure it stands in for is cited beside it as file:line.  A Fortran host binds these with
+ * iso_c_binding (see the shim in INTEGRATION.md); Python binds them with ctypes.
+ *
+ * Conventions
+ *  - Arrays are Fortran-ordered (column-major) and contiguous: a field is f(n1,n2,n3), a state is
+ *    q(n1,n2,n3,5) holding (rho, rho*u, rho*v, rho*w, p) -- src/data/data_rhs.f90:3-4.
+ *  - Functions without a suffix take HOST pointers; they copy in, run on the context's stream and
+ *    copy out before returning.  Functions ending in _dev take DEVICE pointers (on the context's
+ *    device) and only enqueue work on the context's stream (cruna_sync waits for it).
+ *  - Every function returns 0 on success and a negative CRUNA_ERR_* code on failure;
+ *    cruna_last_error() gives the message.  The reference prints and calls stop_cruna instead
+ *    (src/parallelism/mpi_cartesian.f90:327-336); a Fortran shim maps a non-zero status to stop_cruna.
+ *  - One context = one device, one CUDA stream, one grid; a context is not thread-safe (the
+ *    reference keeps the same state in module SAVE variables).
+ */
+#ifndef CRUNA_B200_H
+#define CRUNA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CRUNA_ABI_VERSION 1
+
+/* status codes */
+#define CRUNA_OK 0
+#define CRUNA_ERR_ARG (-1)       /* invalid argument, shape or configuration */
+#define CRUNA_ERR_CUDA (-2)      /* a CUDA runtime call failed */
+#define CRUNA_ERR_NOMEM (-3)     /* device allocation failed */
+#define CRUNA_ERR_STATE (-4)     /* non-finite or non-physical state detected (rho <= 0, p <= 0, NaN) */
+#define CRUNA_ERR_UNSUPPORTED (-5) /* boundary type / scheme / path not available */
+#define CRUNA_ERR_NODEVICE (-6)  /* no CUDA device */
+
+/* derivative cores (selected at compile time in CRUNA by discretisation_x_core.f90) */
+enum cruna_diff_scheme {
+  CRUNA_DIFF_EMPTY = 0,          /* src/diff/diff_pen_core_empty.f90 */
+  CRUNA_DIFF_O2_E_C_O = 1,       /* src/diff/diff_pen_core_o2_e_c_o.f90 */
+  CRUNA_DIFF_O4_E_C_P = 2,       /* src/diff/diff_pen_core_o4_e_c_p.f90 */
+  CRUNA_DIFF_O4_E_C_O = 3,       /* src/diff/diff_pen_core_o4_e_c_o.f90 */
+  CRUNA_DIFF_O4_I_C_P_PADE = 4,  /* src/diff/diff_pen_core_o4_i_c_p_pade.f90 */
+  CRUNA_DIFF_O4_I_C_O_PADE = 5,  /* src/diff/diff_pen_core_o4_i_c_o_pade.f90 */
+  CRUNA_DIFF_O6_I_C_P = 6,       /* src/diff/diff_pen_core_o6_i_c_p.f90 */
+  CRUNA_DIFF_O6_I_C_O = 7,       /* src/diff/diff_pen_core_o6_i_c_o.f90 */
+  CRUNA_DIFF_O8_E_C_P = 8        /* no reference counterpart: 8th-order explicit central, periodic */
+};
+
+/* filter cores (filter_x_core.f90 selector in CRUNA) */
+enum cruna_filter_scheme {
+  CRUNA_FILTER_EMPTY = 0,        /* src/filter/filter_pen_core_empty.f90 */
+  CRUNA_FILTER_O2_I_C_P = 1,     /* src/filter/filter_pen_core_o2_i_c_p.f90 */
+  CRUNA_FILTER_O6_I_C_P = 2,     /* src/filter/filter_pen_core_o6_i_c_p.f90 */
+  CRUNA_FILTER_O2_I_C_O = 3,     /* src/filter/filter_pen_core_o2_i_c_o.f90 */
+  CRUNA_FILTER_O4_I_C_O = 4,     /* src/filter/filter_pen_core_o4_i_c_o.f90 */
+  CRUNA_FILTER_O6_I_C_O = 5,     /* src/filter/filter_pen_core_o6_i_c_o.f90 */
+  CRUNA_FILTER_O8_I_C_O = 6,     /* src/filter/filter_pen_core_o8_i_c_o.f90 */
+  CRUNA_FILTER_O10_I_C_O = 7,    /* src/filter/filter_pen_core_o10_i_c_o.f90 */
+  CRUNA_FILTER_O10_E_C_P = 8     /* no reference counterpart: explicit 10th-order periodic, blended */
+};
+
+/* arithmetic of the stencil / flux / filter work (the RK accumulation is FP64 in both) */
+enum cruna_precision {
+  CRUNA_FP64 = 0,                /* plain path: everything FP64 */
+  CRUNA_FP32_STENCIL = 1         /* stencils, fluxes and filters in FP32 on FP64-stored state */
+};
+
+/*
+ * Solver configuration: the hot-path keys of parameter.dat (src/parameter/parameter.f90:100-170,
+ * ns_rho_rhou_p_trafos.f90, filter cores, shape_functions.f90) as one struct.
+ */
+typedef struct cruna_config {
+  int32_t abi_version;           /* must be CRUNA_ABI_VERSION */
+  int32_t n[3];                  /* geom.n1, geom.n2, geom.n3 */
+  double x0[3];                  /* geom.x10, geom.x20, geom.x30 */
+  double x1[3];                  /* geom.x11, geom.x21, geom.x31 */
+  int32_t diff[3];               /* enum cruna_diff_scheme per direction */
+  int32_t filter[3];             /* enum cruna_filter_scheme per direction */
+  double filter_alpha;           /* filter.alpha */
+  double filter_strength;        /* blend strength of CRUNA_FILTER_O10_E_C_P */
+  int32_t di_freq[3];            /* filter.di1freq..di3freq (direct loop), <= 0 means never */
+  int32_t ai_freq[3];            /* filter.ai1freq..ai3freq (adjoint loop), <= 0 means never */
+  double gamma, R, W, mu0, T0, Pr; /* material.* */
+  double dt;                     /* time.dt */
+  int32_t heat_flux_dx;          /* 0: as the reference, heat-flux Dx calls use dx=1
+                                    (ns_rho_rhou_p.f90:189-197); 1: scale them by the grid spacing */
+  int32_t precision;             /* enum cruna_precision */
+  double sponge_length[3];       /* sponge.length(1..3); <= 0 disables that direction */
+  double sponge_amplitude;       /* sponge.amplitude */
+  int32_t sponge_shape;          /* sponge.shape: 0 quadratic, 1 cos */
+  int32_t device;                /* CUDA device ordinal */
+  int32_t check_every;           /* >0: run-loops check rho>0, p>0, finiteness every N steps */
+} cruna_config;
+
+typedef struct cruna_ctx cruna_ctx;
+
+/* Fills *cfg with the reference's defaults (material.R = 8.3144598, W = 0.0289647, T0 = 273,
+   Pr = 0.71, filter.alpha = 0.35, sponge length 0.3, amplitude 1, quadratic, ...). */
+void cruna_config_defaults(cruna_config *cfg);
+
+/*
+ * Create a context: grid, dx rule (src/geometry/grid_transform.f90:40-56), LAPACK-identical
+ * tridiagonal factors of every compact core (the SAVE'd dgttrf factors, e.g.
+ * diff_pen_core_o6_i_c_p.f90:170-228), the sponge shape (shape_functions.f90:69-150) and the
+ * boundary table.  bc_table holds nbc rows of 10 doubles
+ * (type, is, ie, js, je, ks, ke, k1, k2, k3) with 1-based inclusive global indices, i.e.
+ * boundary_conditions_array after init_boundary_conditions_array / modify_boundary_conditions_array
+ * (boundary_conditions.f90:461-610).  Supported types: 0, 100, 200, 201, 204, 400, 401.
+ */
+int cruna_init(const cruna_config *cfg, const double *bc_table, int nbc, cruna_ctx **out);
+void cruna_free(cruna_ctx *ctx);
+const char *cruna_last_error(const cruna_ctx *ctx);   /* ctx may be NULL (init failures) */
+int cruna_sync(cruna_ctx *ctx);
+int cruna_get_dx(const cruna_ctx *ctx, double dx[3]);
+/* The context's cudaStream_t as an opaque pointer (for callers that interleave their own work). */
+void *cruna_stream(cruna_ctx *ctx);
+
+/* data_reference qref (src/data/data_reference.f90): target of BC 201/204 and the sponges. */
+int cruna_set_reference(cruna_ctx *ctx, const double *qref);
+int cruna_set_reference_dev(cruna_ctx *ctx, const double *qref);
+
+/* apply_force(rhs) (src/opt/force.f90:27-31): rhs += f after the interior RHS; f (n1,n2,n3,5);
+   NULL clears the forcing. */
+int cruna_set_forcing(cruna_ctx *ctx, const double *f);
+int cruna_set_forcing_dev(cruna_ctx *ctx, const double *f);
+
+/* Dx1/Dx2/Dx3(q_x, q, h) (src/diff/diff_i1_mpi_cartesian.f90:17-132) on nfields consecutive fields;
+   dir = 1, 2 or 3; h <= 0 or NaN means "h not present" (dx = 1.0, diff_i1_mpi_cartesian.f90:93-97). */
+int cruna_diff(cruna_ctx *ctx, int dir, const double *in, double *out, int nfields, double h);
+int cruna_diff_dev(cruna_ctx *ctx, int dir, const double *in, double *out, int nfields, double h);
+
+/* filter_i1/2/3(q) (src/filter/filter_i1_mpi_cartesian.f90:18-97) in place on nfields fields. */
+int cruna_filter(cruna_ctx *ctx, int dir, double *q, int nfields);
+int cruna_filter_dev(cruna_ctx *ctx, int dir, double *q, int nfields);
+
+/* right_hand_side_direct_3d(rhs, q_in, t) -- src/equations/ns_rho_rhou_p.f90:31-253 */
+int cruna_rhs_direct(cruna_ctx *ctx, const double *q, double *rhs, double t);
+int cruna_rhs_direct_dev(cruna_ctx *ctx, const double *q, double *rhs, double t);
+
+/* right_hand_side_adjoint_3d(rhs, qs_in, q, g, t) -- ns_rho_rhou_p.f90:257-536 (continuous,
+   inviscid adjoint as in CRUNA); g may be NULL (zero). */
+int cruna_rhs_adjoint(cruna_ctx *ctx, const double *qs, const double *q, const double *g,
+                      double *rhs, double t);
+int cruna_rhs_adjoint_dev(cruna_ctx *ctx, const double *qs, const double *q, const double *g,
+                          double *rhs, double t);
+
+/* time_stepper_direct(q1, q0, t) -- src/time/rk_o4_e.f90:17-58 (classical RK4) */
+int cruna_step_direct(cruna_ctx *ctx, const double *q0, double *q1, double t);
+int cruna_step_direct_dev(cruna_ctx *ctx, const double *q0, double *q1, double t);
+
+/* time_stepper_adjoint(qs1, qs0, q0, g, t) -- rk_o4_e.f90:62-105 (dt -> -dt, q0 frozen) */
+int cruna_step_adjoint(cruna_ctx *ctx, const double *qs0, const double *q0, const double *g,
+                       double *qs1, double t);
+int cruna_step_adjoint_dev(cruna_ctx *ctx, const double *qs0, const double *q0, const double *g,
+                           double *qs1, double t);
+
+/* set_boundary_condition_q(q, outside_rhs)      boundary_conditions.f90:52-136
+   set_boundary_condition_qs(qs, q, outside_rhs) boundary_conditions.f90:140-224
+   set_boundary_condition_rhs(rhs, q)            boundary_conditions.f90:228-298
+   set_boundary_condition_rhss(rhss, qs, q)      boundary_conditions.f90:302-377 (q may be NULL,
+                                                 as in the NS adjoint RHS; a 400 sponge is then off) */
+int cruna_bc_q(cruna_ctx *ctx, double *q, int outside_rhs);
+int cruna_bc_qs(cruna_ctx *ctx, double *qs, const double *q, int outside_rhs);
+int cruna_bc_rhs(cruna_ctx *ctx, double *rhs, const double *q);
+int cruna_bc_rhss(cruna_ctx *ctx, double *rhss, const double *qs, const double *q);
+int cruna_bc_q_dev(cruna_ctx *ctx, double *q, int outside_rhs);
+int cruna_bc_qs_dev(cruna_ctx *ctx, double *qs, const double *q, int outside_rhs);
+int cruna_bc_rhs_dev(cruna_ctx *ctx, double *rhs, const double *q);
+int cruna_bc_rhss_dev(cruna_ctx *ctx, double *rhss, const double *qs, const double *q);
+
+/*
+ * Loop body of calc_direct (src/main/computation_direct.f90:64-107), nsteps steps starting after
+ * step nt0: time_stepper_direct -> set_boundary_condition_q(outside_rhs) -> filter_i1/2/3 when
+ * mod(nt, di_freq) == 0.  q_io holds q0 on entry and q(nt0+nsteps) on return.  traj, if not NULL,
+ * receives the state after every step: traj[(s)*N*5 ...] for s = 0..nsteps-1 (the Q(:,:,:,:,nt)
+ * store of computation_direct.f90:102).
+ */
+int cruna_run_direct(cruna_ctx *ctx, double *q_io, int nt0, int nsteps, double *traj);
+int cruna_run_direct_dev(cruna_ctx *ctx, double *q_io, int nt0, int nsteps, double *traj);
+
+/*
+ * Loop body of calc_adjoint (src/main/computation_adjoint.f90:60-108) for nt = nt_end..nt_end-nsteps+1:
+ * q0 = Q(nt), g = calc_objective_g(q0) (here: the caller's g_traj slice or zero), adjoint step,
+ * set_boundary_condition_qs(outside_rhs), filters when mod(nt, ai_freq) == 0.  Q_traj holds the
+ * direct states Q(nt_end-nsteps+1 .. nt_end) in that order; g_traj the matching sources (or NULL).
+ */
+int cruna_run_adjoint(cruna_ctx *ctx, double *qs_io, const double *Q_traj, const double *g_traj,
+                      int nt_end, int nsteps);
+int cruna_run_adjoint_dev(cruna_ctx *ctx, double *qs_io, const double *Q_traj, const double *g_traj,
+                          int nt_end, int nsteps);
+
+/* State check used by the run loops: returns CRUNA_ERR_STATE if any rho <= 0, p <= 0 or a
+   non-finite value is found in q (device pointer). */
+int cruna_check_state_dev(cruna_ctx *ctx, const double *q);
+
+/* Which RHS implementation the context uses: 1 = fused explicit kernels, 0 = generic line-operator
+   sequence (compact schemes, 204/200 boundary types).  force_generic=1 selects the generic one. */
+int cruna_rhs_path(const cruna_ctx *ctx);
+int cruna_set_force_generic(cruna_ctx *ctx, int force_generic);
+
+/* Number of kernels this library enqueued since the context was created (for launch accounting). */
+int64_t cruna_kernel_launches(const cruna_ctx *ctx);
+
+/* The library's restatement of LAPACK dgttrf / dgttrs('N', nrhs=1), which every compact core of the
+   reference calls (e.g. diff_pen_core_o6_i_c_p.f90:135,213,219); exported so callers and tests can
+   compare its factors with their LAPACK.  ipiv is 1-based as in LAPACK. */
+int cruna_lapack_dgttrf(int n, double *dl, double *d, double *du, double *du2, int *ipiv);
+void cruna_lapack_dgttrs(int n, const double *dl, const double *d, const double *du, const double *du2,
+                         const int *ipiv, double *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CRUNA_B200_H */

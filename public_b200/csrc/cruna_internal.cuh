@@ -1,0 +1,154 @@
+// Internal declarations of the CRUNA B200 library: line operators, context, kernel launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cruna_b200.h"
+
+namespace cruna {
+
+constexpr int kMaxR = 6;        // largest interior half-width (o10 filter: 5)
+constexpr int kMaxRows = 5;     // largest number of explicit boundary rows at one end
+constexpr int kMaxRowW = 12;    // widest boundary row (o10 filter: 11 points)
+
+enum OpKind { OP_ZERO = 0, OP_COPY = 1, OP_STENCIL = 2 };
+
+// One direction's derivative or filter operator on lines of n points: an explicit stencil part
+// (interior + optional one-sided rows at both ends, or periodic wrap), optionally followed by a
+// tridiagonal solve with LAPACK dgttrf factors and a Sherman-Morrison cyclic correction -- the
+// structure shared by every src/diff/diff_pen_core_* and src/filter/filter_pen_core_* module.
+struct LineOp {
+  int n = 1;
+  int kind = OP_ZERO;
+  int periodic = 0;
+  int antisym = 0;                 // 1: derivative (end rows mirror with a sign flip)
+  int r = 0;                       // interior half-width
+  double c[kMaxR + 1] = {0};       // interior coefficients c[0..r] (c[0] unused when antisym)
+  int nb = 0;                      // explicit rows at each end (open lines)
+  int bw = 0;                      // width of those rows
+  int keep_ends = 0;               // row 0 copies the input (open filters)
+  double brow[kMaxRows][kMaxRowW] = {{0}};
+  double div = 1.0;                // explicit part is divided by (h * div): 12 for o4 explicit
+  int solve = 0;                   // dgttrs follows
+  int cyclic = 0;                  // Sherman-Morrison correction follows
+  double blend = 0.0;              // >0: out = q - blend * (q - F q)
+  double fbrat = 0.0;
+  // device factor arrays (owned by the context)
+  const double *dl = nullptr, *inv_d = nullptr, *du = nullptr, *du2 = nullptr, *fbnorm = nullptr;
+  const int *ipiv = nullptr;
+};
+
+// Host-side copy of the factors (filled by the dgttrf restatement in schemes.cpp).
+struct HostFactors {
+  std::vector<double> dl, d, du, du2, fbnorm;
+  std::vector<int> ipiv;  // 1-based as LAPACK
+  double fbrat = 0.0;
+  int info = 0;
+};
+
+struct Grid {
+  int n1, n2, n3;
+  long long N;   // points per field
+};
+
+// builds the operators (schemes.cpp); return false + message on unsupported input
+bool build_diff_op(int scheme, int n, LineOp &op, HostFactors &hf, std::string &err);
+bool build_filter_op(int scheme, int n, double alpha, double strength, LineOp &op, HostFactors &hf,
+                     std::string &err);
+bool diff_is_periodic(int scheme);
+// LAPACK dgttrf / dgttrs (no transpose) restated (schemes.cpp); exposed for tests through the C API
+int lapack_dgttrf(int n, double *dl, double *d, double *du, double *du2, int *ipiv);
+void lapack_dgttrs(int n, const double *dl, const double *d, const double *du, const double *du2,
+                   const int *ipiv, double *b);
+
+struct BCRow {
+  int type;
+  int is, ie, js, je, ks, ke;  // 0-based inclusive
+  double k[3];
+  int comp;                    // wall component (0-based)
+  int shift[3];                // type 200: offset of the aim plane
+};
+
+// device sponge-shape factors: phi = (((sx[i]*sym[j])*syp[j])*szm[k])*szp[k]; shape = amp*(1-phi)
+struct SpongeDev {
+  const double *sx = nullptr, *sym = nullptr, *syp = nullptr, *szm = nullptr, *szp = nullptr;
+  double amp = 0.0;
+};
+
+}  // namespace cruna
+
+struct cruna_ctx {
+  cruna_config cfg;
+  cruna::Grid g;
+  double dx[3];
+  cruna::LineOp dop[3];   // derivative operators
+  cruna::LineOp fop[3];   // filter operators
+  std::vector<cruna::BCRow> bc;
+  bool has_q_bc = false, has_rhs_bc = false, has_sponge = false, has_nonlocal_bc = false;
+  cruna::SpongeDev sponge;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  int64_t launches = 0;
+  std::string err;
+  bool force_generic = false;
+  bool fused_ok = false;
+  // device memory
+  std::vector<void *> allocations;
+  double *qref = nullptr;        // 5N
+  double *force = nullptr;       // 5N or null
+  double *st[6] = {nullptr};     // state-sized work buffers
+  double *io[4] = {nullptr};     // staging for host-pointer entry points (5N each)
+  double *tmp = nullptr;         // generic-path temporaries (kGenericFields * N)
+  double *fz = nullptr;          // fused-path intermediates
+  float *fz32 = nullptr;         // fused-path FP32 intermediates
+  double *red = nullptr;         // reduction scratch
+  int *flag = nullptr;           // device error flag
+};
+
+namespace cruna {
+
+// launch helpers (ops.cu)
+void launch_line_stencil(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
+                         double *out, double scale, int nfields, double sign = 1.0);
+void launch_line_solve(cruna_ctx *c, const LineOp &op, int dir, double *data, int nfields);
+void apply_diff(cruna_ctx *c, int dir, const double *f1, const double *f2, double *out, double h,
+                int nfields);
+void apply_filter(cruna_ctx *c, int dir, double *q, double *scratch, int nfields);
+
+// RHS / BC / RK (ops.cu, fused.cu)
+void rhs_direct_generic(cruna_ctx *c, const double *q, double *rhs, double *qbc_scratch);
+void rhs_adjoint_generic(cruna_ctx *c, const double *qs, const double *q, const double *g, double *rhs,
+                         double *qsbc_scratch);
+bool fused_supported(const cruna_ctx *c);
+void rhs_direct_fused(cruna_ctx *c, const double *q, double *rhs, int stage, const double *q0,
+                      double *acc, double *qnext, double dt);
+void bc_q(cruna_ctx *c, double *q, int outside);
+void bc_qs(cruna_ctx *c, double *qs, const double *q, int outside);
+void bc_rhs(cruna_ctx *c, double *rhs, const double *q);
+void bc_rhss(cruna_ctx *c, double *rhss, const double *qs, const double *q);
+void rk_stage(cruna_ctx *c, int stage, double dt, const double *k, const double *q0, double *acc,
+              double *qnext);
+void copy_state(cruna_ctx *c, double *dst, const double *src, int nfields);
+int check_state(cruna_ctx *c, const double *q);
+void add_fields(cruna_ctx *c, double *dst, const double *src, long long n);
+
+}  // namespace cruna
+
+#define CRUNA_CUDA_CHECK(call)                                                     \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e_) \
+                               + " at " + __FILE__ + ":" + std::to_string(__LINE__)); \
+    }                                                                              \
+  } while (0)
+
+#define CRUNA_LAUNCH_CHECK(ctx)                                                   \
+  do {                                                                            \
+    (ctx)->launches++;                                                            \
+    CRUNA_CUDA_CHECK(cudaGetLastError());                                         \
+  } while (0)

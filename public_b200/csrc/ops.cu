@@ -1,0 +1,763 @@
+// Generic kernels of the CRUNA B200 library: line operators (derivatives and filters of any
+// reference scheme along any direction), boundary conditions, RK4 stage updates and the generic
+// RHS sequences that mirror src/equations/ns_rho_rhou_p.f90 call by call.
+#include <cmath>
+#include <stdexcept>
+#include <string>
+
+#include "cruna_internal.cuh"
+
+namespace cruna {
+
+constexpr int kThreads = 256;
+
+static inline int nblocks(long long work, int threads = kThreads) {
+  long long b = (work + threads - 1) / threads;
+  return (int)(b < 1 ? 1 : b);
+}
+
+// ------------------------------------------------------------------------------------------------
+// line operators
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void line_geom(const Grid &g, int dir, long long p, long long &base,
+                                          long long &stride, int &i) {
+  // p is a point index inside one field; returns the line base offset, stride and position
+  const long long n1 = g.n1, n12 = (long long)g.n1 * g.n2;
+  const long long ii = p % n1, jj = (p / n1) % g.n2, kk = p / n12;
+  if (dir == 0) { i = (int)ii; stride = 1; base = p - ii; }
+  else if (dir == 1) { i = (int)jj; stride = n1; base = p - jj * n1; }
+  else { i = (int)kk; stride = n12; base = p - kk * n12; }
+}
+
+__device__ __forceinline__ double ldv(const double *f1, const double *f2, long long idx) {
+  return f2 ? f1[idx] * f2[idx] : f1[idx];
+}
+
+// explicit part of the operator at position i of the line starting at f + base
+__device__ double explicit_part(const LineOp &op, const double *f1, const double *f2, long long base,
+                                long long s, int i) {
+  const int n = op.n;
+  if (op.kind == OP_ZERO) return 0.0;
+  if (op.kind == OP_COPY) return ldv(f1, f2, base + i * s);
+  if (op.periodic) {
+    if (op.antisym) {
+      double t = 0.0;
+      for (int m = 1; m <= op.r; ++m) {
+        int ip = (i + m) % n, im = ((i - m) % n + n) % n;
+        double d = ldv(f1, f2, base + ip * s) - ldv(f1, f2, base + im * s);
+        t = (m == 1) ? op.c[1] * d : t + op.c[m] * d;
+      }
+      return t;
+    }
+    double t = op.c[0] * ldv(f1, f2, base + i * s);
+    for (int m = 1; m <= op.r; ++m) {
+      int ip = (i + m) % n, im = ((i - m) % n + n) % n;
+      t = t + op.c[m] * (ldv(f1, f2, base + ip * s) + ldv(f1, f2, base + im * s));
+    }
+    return t;
+  }
+  if (i >= op.nb && i < n - op.nb) {
+    if (op.antisym) {
+      double t = 0.0;
+      for (int m = 1; m <= op.r; ++m) {
+        double d = ldv(f1, f2, base + (i + m) * s) - ldv(f1, f2, base + (i - m) * s);
+        t = (m == 1) ? op.c[1] * d : t + op.c[m] * d;
+      }
+      return t;
+    }
+    double t = op.c[0] * ldv(f1, f2, base + i * s);
+    for (int m = 1; m <= op.r; ++m)
+      t = t + op.c[m] * (ldv(f1, f2, base + (i + m) * s) + ldv(f1, f2, base + (i - m) * s));
+    return t;
+  }
+  const bool start = i < op.nb;
+  const int row = start ? i : n - 1 - i;
+  if (op.keep_ends && row == 0) return ldv(f1, f2, base + i * s);
+  double t = 0.0;
+  for (int m = 0; m < op.bw; ++m) {
+    const int j = start ? m : n - 1 - m;
+    t = (m == 0) ? op.brow[row][0] * ldv(f1, f2, base + j * s)
+                 : t + op.brow[row][m] * ldv(f1, f2, base + j * s);
+  }
+  return (op.antisym && !start) ? -t : t;
+}
+
+__global__ void k_line_stencil(LineOp op, Grid g, int dir, const double *__restrict__ f1,
+                               const double *__restrict__ f2, double *__restrict__ out, double scale,
+                               double sign, int nfields) {
+  const long long total = g.N * nfields;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long fld = t / g.N, p = t - fld * g.N;
+    long long base, s;
+    int i;
+    line_geom(g, dir, p, base, s, i);
+    const double *a = f1 + fld * g.N;
+    const double *b = f2 ? f2 + fld * g.N : nullptr;
+    double v = explicit_part(op, a, b, base, s, i);
+    if (op.kind == OP_STENCIL && op.antisym) v = v * scale;
+    if (op.blend > 0.0) {
+      const double q = ldv(a, b, p);
+      v = q - op.blend * (q - v);
+    }
+    out[t] = sign * v;
+  }
+}
+
+// one thread per line: dgttrs('N') sweeps (pivots as LAPACK) + cyclic correction, in place
+__global__ void k_line_solve(LineOp op, Grid g, int dir, double *__restrict__ data, int nfields) {
+  const int n = op.n;
+  const long long nlines = g.N / n;
+  const long long total = nlines * nfields;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long fld = t / nlines, l = t - fld * nlines;
+    long long base, s;
+    if (dir == 0) { base = l * g.n1; s = 1; }
+    else if (dir == 1) { const long long i = l % g.n1, k = l / g.n1; base = i + k * (long long)g.n1 * g.n2; s = g.n1; }
+    else { base = l; s = (long long)g.n1 * g.n2; }
+    double *b = data + fld * g.N + base;
+    for (int i = 0; i < n - 1; ++i) {
+      if (op.ipiv[i] == i + 1) {
+        b[(i + 1) * s] = b[(i + 1) * s] - op.dl[i] * b[i * s];
+      } else {
+        const double temp = b[i * s];
+        const double nxt = b[(i + 1) * s];
+        b[i * s] = nxt;
+        b[(i + 1) * s] = temp - op.dl[i] * nxt;
+      }
+    }
+    double x2 = b[(n - 1) * s] * op.inv_d[n - 1];
+    b[(n - 1) * s] = x2;
+    double x1 = x2;
+    if (n > 1) {
+      x1 = (b[(n - 2) * s] - op.du[n - 2] * x2) * op.inv_d[n - 2];
+      b[(n - 2) * s] = x1;
+    }
+    for (int i = n - 3; i >= 0; --i) {
+      const double x0 = (b[i * s] - op.du[i] * x1 - op.du2[i] * x2) * op.inv_d[i];
+      b[i * s] = x0;
+      x2 = x1;
+      x1 = x0;
+    }
+    if (op.cyclic) {
+      const double corr = b[0] + op.fbrat * b[(n - 1) * s];
+      for (int i = 0; i < n; ++i) b[i * s] = b[i * s] - op.fbnorm[i] * corr;
+    }
+  }
+}
+
+void launch_line_stencil(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
+                         double *out, double scale, int nfields, double sign) {
+  const long long work = c->g.N * nfields;
+  const int blocks = (int)std::min<long long>(nblocks(work), 148LL * 64);
+  k_line_stencil<<<blocks, kThreads, 0, c->stream>>>(op, c->g, dir, f1, f2, out, scale, sign, nfields);
+  CRUNA_LAUNCH_CHECK(c);
+}
+
+void launch_line_solve(cruna_ctx *c, const LineOp &op, int dir, double *data, int nfields) {
+  const long long lines = (c->g.N / op.n) * nfields;
+  k_line_solve<<<nblocks(lines, 128), 128, 0, c->stream>>>(op, c->g, dir, data, nfields);
+  CRUNA_LAUNCH_CHECK(c);
+}
+
+// Dx_d of f1 (or of f1*f2): explicit part scaled by 1/(h*div), then the compact solve if any
+void apply_diff(cruna_ctx *c, int dir, const double *f1, const double *f2, double *out, double h,
+                int nfields) {
+  const LineOp &op = c->dop[dir];
+  const double scale = 1.0 / (h * op.div);
+  launch_line_stencil(c, op, dir, f1, f2, out, scale, nfields);
+  if (op.kind == OP_STENCIL && op.solve) launch_line_solve(c, op, dir, out, nfields);
+}
+
+// filter_i_d in place: out-of-place stencil into scratch, solve, copy back
+void apply_filter(cruna_ctx *c, int dir, double *q, double *scratch, int nfields) {
+  const LineOp &op = c->fop[dir];
+  if (op.kind == OP_COPY) return;
+  launch_line_stencil(c, op, dir, q, nullptr, scratch, 1.0, nfields);
+  if (op.solve) launch_line_solve(c, op, dir, scratch, nfields);
+  CRUNA_CUDA_CHECK(cudaMemcpyAsync(q, scratch, sizeof(double) * c->g.N * nfields,
+                                   cudaMemcpyDeviceToDevice, c->stream));
+}
+
+// ------------------------------------------------------------------------------------------------
+// sponge shape on the fly: phi = (((sx*sym)*syp)*szm)*szp, shape = amp*(1 - phi)
+// (src/boundaries/shape_functions.f90:104-145)
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double sponge_at(const SpongeDev &sp, const Grid &g, long long p) {
+  const long long i = p % g.n1, j = (p / g.n1) % g.n2, k = p / ((long long)g.n1 * g.n2);
+  double phi = sp.sx[i] * sp.sym[j];
+  phi = phi * sp.syp[j];
+  phi = phi * sp.szm[k];
+  phi = phi * sp.szp[k];
+  return sp.amp * (1.0 - phi);
+}
+
+// ------------------------------------------------------------------------------------------------
+// boundary kernels
+// ------------------------------------------------------------------------------------------------
+struct Box {
+  int is, ie, js, je, ks, ke;
+  __host__ __device__ long long count() const { return (long long)(ie - is + 1) * (je - js + 1) * (ke - ks + 1); }
+};
+
+__device__ __forceinline__ long long box_point(const Box &b, const Grid &g, long long t, int &i, int &j,
+                                               int &k) {
+  const int ni = b.ie - b.is + 1, nj = b.je - b.js + 1;
+  i = b.is + (int)(t % ni);
+  j = b.js + (int)((t / ni) % nj);
+  k = b.ks + (int)(t / ((long long)ni * nj));
+  return i + (long long)g.n1 * (j + (long long)g.n2 * k);
+}
+
+// characteristic_q_k1d (src/boundaries/nonreflecting.f90:46-137) -- aim from `aim` at p + aim_off
+__global__ void k_char_q(Box b, Grid g, double k1, double k2, double k3, double gamma, double *q,
+                         const double *aim, long long aim_off) {
+  const long long tot = b.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    const long long p = box_point(b, g, t, i, j, k);
+    const long long N = g.N, pa = p + aim_off;
+    const double r = q[p], u0 = q[p + N] / r, u1 = q[p + 2 * N] / r, u2 = q[p + 3 * N] / r, pp = q[p + 4 * N];
+    const double c = sqrt(gamma * q[p + 4 * N] / q[p]);
+    const double ar = aim[pa];
+    const double d0 = ar - r;
+    const double d1 = aim[pa + N] / ar - u0;
+    const double d2 = aim[pa + 2 * N] / ar - u1;
+    const double d3 = aim[pa + 3 * N] / ar - u2;
+    const double d4 = aim[pa + 4 * N] - pp;
+    const double kx = -k1, ky = -k2, kz = -k3;
+    const double c2 = c * c;
+    double R1 = kx * d0 + kz * d2 - ky * d3 - kx * d4 / c2;
+    double R2 = ky * d0 - kz * d1 + kx * d3 - ky * d4 / c2;
+    double R3 = kz * d0 + ky * d1 - kx * d2 - kz * d4 / c2;
+    double R4 = kx * d1 + ky * d2 + kz * d3 + d4 / (r * c);
+    double R5 = -kx * d1 - ky * d2 - kz * d3 + d4 / (r * c);
+    const double lamS = kx * u0 + ky * u1 + kz * u2;
+    const double lamP = lamS + c, lamM = lamS - c;
+    if (lamS < 0.0) { R1 = 0.0; R2 = 0.0; R3 = 0.0; }
+    if (lamP < 0.0) R4 = 0.0;
+    if (lamM < 0.0) R5 = 0.0;
+    const double e1 = kx * R1 + ky * R2 + kz * R3 + r / (2.0 * c) * R4 + r / (2.0 * c) * R5;
+    const double e2 = -kz * R2 + ky * R3 + 0.5 * kx * R4 - 0.5 * kx * R5;
+    const double e3 = kz * R1 - kx * R3 + 0.5 * ky * R4 - 0.5 * ky * R5;
+    const double e4 = -ky * R1 + kx * R2 + 0.5 * kz * R4 - 0.5 * kz * R5;
+    const double e5 = +0.5 * r * c * R4 + 0.5 * r * c * R5;
+    const double rn = r + e1;
+    q[p] = rn;
+    q[p + N] = rn * (u0 + e2);
+    q[p + 2 * N] = rn * (u1 + e3);
+    q[p + 3 * N] = rn * (u2 + e4);
+    q[p + 4 * N] = pp + e5;
+  }
+}
+
+// characteristic_qs_k1d (nonreflecting.f90:453-554); q sampled at p + q_off
+__global__ void k_char_qs(Box b, Grid g, double k1, double k2, double k3, double gamma, double *qs,
+                          const double *q, long long q_off) {
+  const long long tot = b.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    const long long p = box_point(b, g, t, i, j, k);
+    const long long N = g.N, pq = p + q_off;
+    const double ds0 = -qs[p], ds1 = -qs[p + N], ds2 = -qs[p + 2 * N], ds3 = -qs[p + 3 * N],
+                 ds4 = -qs[p + 4 * N];
+    const double kx = -k1, ky = -k2, kz = -k3;
+    const double gm1 = gamma - 1.0;
+    const double c = sqrt(gamma * (q[pq + 4 * N] / q[pq]));
+    const double g_c = gm1 / c;
+    const double u = q[pq + N] / q[pq], v = q[pq + 2 * N] / q[pq], w = q[pq + 3 * N] / q[pq];
+    const double ku = kx * u + ky * v + kz * w;
+    const double kus = kx * ds1 + ky * ds2 + kz * ds3;
+    const double ruus = (ds0 + u * ds1 + v * ds2 + w * ds3) / c;
+    const double rups = ruus + ds4 / g_c;
+    double drs = 0.0, dus = 0.0, dvs = 0.0, dws = 0.0, dps = 0.0;
+    if (ku < 0.0) {
+      drs = ds0 + ku * kus;
+      dus = ds1 - kx * kus;
+      dvs = ds2 - ky * kus;
+      dws = ds3 - kz * kus;
+      dps = -g_c * ruus;
+    }
+    if (ku + c < 0.0) {
+      const double tmp = 0.5 * (kus + rups);
+      drs = drs - ku * tmp; dus = dus + kx * tmp; dvs = dvs + ky * tmp; dws = dws + kz * tmp;
+      dps = dps + g_c * tmp;
+    }
+    if (ku - c < 0.0) {
+      const double tmp = 0.5 * (kus - rups);
+      drs = drs - ku * tmp; dus = dus + kx * tmp; dvs = dvs + ky * tmp; dws = dws + kz * tmp;
+      dps = dps - g_c * tmp;
+    }
+    qs[p] = qs[p] + drs;
+    qs[p + N] = qs[p + N] + dus;
+    qs[p + 2 * N] = qs[p + 2 * N] + dvs;
+    qs[p + 3 * N] = qs[p + 3 * N] + dws;
+    qs[p + 4 * N] = qs[p + 4 * N] + dps;
+  }
+}
+
+// characteristic_rhs_k1d without shape (nonreflecting.f90:237-341), BC type 204
+__global__ void k_char_rhs(Box b, Grid g, double k1, double k2, double k3, double gamma, double dt,
+                           double *rhs, const double *q, const double *aim) {
+  const long long tot = b.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    const long long p = box_point(b, g, t, i, j, k);
+    const long long N = g.N;
+    const double inv_dt = 1.0 / dt;
+    const double r = q[p], u0 = q[p + N] / r, u1 = q[p + 2 * N] / r, u2 = q[p + 3 * N] / r;
+    const double c = sqrt(gamma * q[p + 4 * N] / q[p]);
+    const double ar = aim[p];
+    double d0 = ar - r, d1 = aim[p + N] / ar - u0, d2 = aim[p + 2 * N] / ar - u1,
+           d3 = aim[p + 3 * N] / ar - u2, d4 = aim[p + 4 * N] - q[p + 4 * N];
+    const double tmp = dt / r;
+    d0 = d0 + rhs[p] * dt;
+    d1 = d1 + rhs[p + N] * tmp;
+    d2 = d2 + rhs[p + 2 * N] * tmp;
+    d3 = d3 + rhs[p + 3 * N] * tmp;
+    d4 = d4 + rhs[p + 4 * N] * dt;
+    const double kx = -k1, ky = -k2, kz = -k3, c2 = c * c;
+    double R1 = kx * d0 + kz * d2 - ky * d3 - kx * d4 / c2;
+    double R2 = ky * d0 - kz * d1 + kx * d3 - ky * d4 / c2;
+    double R3 = kz * d0 + ky * d1 - kx * d2 - kz * d4 / c2;
+    double R4 = kx * d1 + ky * d2 + kz * d3 + d4 / (r * c);
+    double R5 = -kx * d1 - ky * d2 - kz * d3 + d4 / (r * c);
+    const double lamS = kx * u0 + ky * u1 + kz * u2;
+    if (lamS < 0.0) { R1 = 0.0; R2 = 0.0; R3 = 0.0; }
+    if (lamS + c < 0.0) R4 = 0.0;
+    if (lamS - c < 0.0) R5 = 0.0;
+    const double e1 = kx * R1 + ky * R2 + kz * R3 + r / (2.0 * c) * R4 + r / (2.0 * c) * R5;
+    const double e2 = -kz * R2 + ky * R3 + 0.5 * kx * R4 - 0.5 * kx * R5;
+    const double e3 = kz * R1 - kx * R3 + 0.5 * ky * R4 - 0.5 * ky * R5;
+    const double e4 = -ky * R1 + kx * R2 + 0.5 * kz * R4 - 0.5 * kz * R5;
+    const double e5 = +0.5 * r * c * R4 + 0.5 * r * c * R5;
+    const double rn = r + e1;
+    rhs[p] = e1 * inv_dt;
+    const double t2 = inv_dt * rn;
+    rhs[p + N] = e2 * t2;
+    rhs[p + 2 * N] = e3 * t2;
+    rhs[p + 3 * N] = e4 * t2;
+    rhs[p + 4 * N] = e5 * inv_dt;
+  }
+}
+
+// wall_slip_no_thermodynamics (src/boundaries/wall_boundary_conditions.f90:13-23)
+__global__ void k_wall(Box b, Grid g, int comp, double *rhs) {
+  const long long tot = b.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    const long long p = box_point(b, g, t, i, j, k);
+    rhs[p + comp * g.N] = 0.0;
+  }
+}
+
+// sponge_rhs / sponge_q / sponge_qs / sponge_rhss_correct (src/boundaries/sponge_layer_core.f90)
+__global__ void k_sponge(int mode, Grid g, SpongeDev sp, double gamma, double *a, const double *b,
+                         const double *qref) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double sh = sponge_at(sp, g, p);
+    const long long N = g.N;
+    if (mode == 0) {          // rhs -= shape*(q - qref): a = rhs, b = q
+      for (int v = 0; v < 5; ++v) a[p + v * N] = a[p + v * N] - sh * (b[p + v * N] - qref[p + v * N]);
+    } else if (mode == 1) {   // q -= shape*(q - qref): a = q
+      for (int v = 0; v < 5; ++v) a[p + v * N] = a[p + v * N] - sh * (a[p + v * N] - qref[p + v * N]);
+    } else if (mode == 2) {   // qs -= shape*qs
+      for (int v = 0; v < 5; ++v) a[p + v * N] = a[p + v * N] - sh * a[p + v * N];
+    } else {                  // rhss += shape*(-(A^T)^-1 C^T qs): a = rhss, b = qs, qref = q
+      const double *q = qref;
+      const double rho = q[p];
+      const double u0 = q[p + N] / rho, u1 = q[p + 2 * N] / rho, u2 = q[p + 3 * N] / rho;
+      const double s0 = 1.0 * b[p] - u0 / rho * b[p + N] - u1 / rho * b[p + 2 * N] - u2 / rho * b[p + 3 * N];
+      const double s1 = 1.0 / rho * b[p + N];
+      const double s2 = 1.0 / rho * b[p + 2 * N];
+      const double s3 = 1.0 / rho * b[p + 3 * N];
+      const double s4 = (gamma - 1.0) * b[p + 4 * N];
+      a[p] += sh * s0;
+      a[p + N] += sh * s1;
+      a[p + 2 * N] += sh * s2;
+      a[p + 3 * N] += sh * s3;
+      a[p + 4 * N] += sh * s4;
+    }
+  }
+}
+
+static Box box_of(const BCRow &r) { return Box{r.is, r.ie, r.js, r.je, r.ks, r.ke}; }
+
+static long long offset_of(const cruna_ctx *c, const int sh[3]) {
+  return sh[0] + (long long)c->g.n1 * (sh[1] + (long long)c->g.n2 * sh[2]);
+}
+
+void bc_q(cruna_ctx *c, double *q, int /*outside*/) {
+  for (const BCRow &r : c->bc) {
+    Box b = box_of(r);
+    const int blocks = nblocks(b.count());
+    if (r.type == 200) {
+      k_char_q<<<blocks, kThreads, 0, c->stream>>>(b, c->g, r.k[0], r.k[1], r.k[2], c->cfg.gamma, q, q,
+                                                   offset_of(c, r.shift));
+      CRUNA_LAUNCH_CHECK(c);
+    } else if (r.type == 201) {
+      k_char_q<<<blocks, kThreads, 0, c->stream>>>(b, c->g, r.k[0], r.k[1], r.k[2], c->cfg.gamma, q,
+                                                   c->qref, 0);
+      CRUNA_LAUNCH_CHECK(c);
+    } else if (r.type == 401) {
+      k_sponge<<<nblocks(c->g.N), kThreads, 0, c->stream>>>(1, c->g, c->sponge, c->cfg.gamma, q, nullptr,
+                                                             c->qref);
+      CRUNA_LAUNCH_CHECK(c);
+    }
+  }
+}
+
+void bc_qs(cruna_ctx *c, double *qs, const double *q, int /*outside*/) {
+  for (const BCRow &r : c->bc) {
+    Box b = box_of(r);
+    const int blocks = nblocks(b.count());
+    if (r.type == 200 || r.type == 201) {
+      const long long off = r.type == 200 ? offset_of(c, r.shift) : 0;
+      k_char_qs<<<blocks, kThreads, 0, c->stream>>>(b, c->g, r.k[0], r.k[1], r.k[2], c->cfg.gamma, qs, q,
+                                                    off);
+      CRUNA_LAUNCH_CHECK(c);
+    } else if (r.type == 401) {
+      k_sponge<<<nblocks(c->g.N), kThreads, 0, c->stream>>>(2, c->g, c->sponge, c->cfg.gamma, qs, nullptr,
+                                                             nullptr);
+      CRUNA_LAUNCH_CHECK(c);
+    }
+  }
+}
+
+void bc_rhs(cruna_ctx *c, double *rhs, const double *q) {
+  for (const BCRow &r : c->bc) {
+    Box b = box_of(r);
+    if (r.type == 100) {
+      k_wall<<<nblocks(b.count()), kThreads, 0, c->stream>>>(b, c->g, r.comp, rhs);
+      CRUNA_LAUNCH_CHECK(c);
+    } else if (r.type == 204) {
+      k_char_rhs<<<nblocks(b.count()), kThreads, 0, c->stream>>>(b, c->g, r.k[0], r.k[1], r.k[2],
+                                                                c->cfg.gamma, c->cfg.dt, rhs, q, c->qref);
+      CRUNA_LAUNCH_CHECK(c);
+    } else if (r.type == 400) {
+      k_sponge<<<nblocks(c->g.N), kThreads, 0, c->stream>>>(0, c->g, c->sponge, c->cfg.gamma, rhs, q,
+                                                             c->qref);
+      CRUNA_LAUNCH_CHECK(c);
+    }
+  }
+}
+
+void bc_rhss(cruna_ctx *c, double *rhss, const double *qs, const double *q) {
+  for (const BCRow &r : c->bc) {
+    Box b = box_of(r);
+    if (r.type == 100) {
+      k_wall<<<nblocks(b.count()), kThreads, 0, c->stream>>>(b, c->g, r.comp, rhss);
+      CRUNA_LAUNCH_CHECK(c);
+    } else if (r.type == 400 && q != nullptr) {
+      k_sponge<<<nblocks(c->g.N), kThreads, 0, c->stream>>>(3, c->g, c->sponge, c->cfg.gamma, rhss, qs, q);
+      CRUNA_LAUNCH_CHECK(c);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// RK4 stage update (src/time/rk_o4_e.f90:45-50 and :92-97): q_{s+1} = q0 + c*dt*k and the
+// accumulation k1 + 2k2 + 2k3 + k4, finished by q1 = q0 + dt/6*acc
+// ------------------------------------------------------------------------------------------------
+__global__ void k_rk_stage(int stage, long long M, double dt, const double *__restrict__ k,
+                           const double *__restrict__ q0, double *__restrict__ acc,
+                           double *__restrict__ qn) {
+  const double dth = dt * 0.5;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < M;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double kv = k[p];
+    if (stage == 1) {
+      acc[p] = kv;
+      qn[p] = q0[p] + dth * kv;
+    } else if (stage == 2) {
+      acc[p] = acc[p] + 2.0 * kv;
+      qn[p] = q0[p] + dth * kv;
+    } else if (stage == 3) {
+      acc[p] = acc[p] + 2.0 * kv;
+      qn[p] = q0[p] + dt * kv;
+    } else {
+      qn[p] = q0[p] + dt / 6.0 * (acc[p] + kv);
+    }
+  }
+}
+
+void rk_stage(cruna_ctx *c, int stage, double dt, const double *k, const double *q0, double *acc,
+              double *qnext) {
+  const long long M = c->g.N * 5;
+  k_rk_stage<<<(int)std::min<long long>(nblocks(M), 148LL * 32), kThreads, 0, c->stream>>>(stage, M, dt, k,
+                                                                                           q0, acc, qnext);
+  CRUNA_LAUNCH_CHECK(c);
+}
+
+void copy_state(cruna_ctx *c, double *dst, const double *src, int nfields) {
+  if (dst == src) return;
+  CRUNA_CUDA_CHECK(cudaMemcpyAsync(dst, src, sizeof(double) * c->g.N * nfields, cudaMemcpyDeviceToDevice,
+                                   c->stream));
+}
+
+__global__ void k_add(long long M, double *dst, const double *src) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < M;
+       p += (long long)gridDim.x * blockDim.x)
+    dst[p] = dst[p] + src[p];
+}
+
+void add_fields(cruna_ctx *c, double *dst, const double *src, long long n) {
+  k_add<<<(int)std::min<long long>(nblocks(n), 148LL * 32), kThreads, 0, c->stream>>>(n, dst, src);
+  CRUNA_LAUNCH_CHECK(c);
+}
+
+// state check: flag bit 1 = non-finite, bit 2 = rho <= 0, bit 4 = p <= 0
+__global__ void k_check(long long N, const double *q, int *flag) {
+  int f = 0;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    for (int v = 0; v < 5; ++v)
+      if (!isfinite(q[p + v * N])) f |= 1;
+    if (!(q[p] > 0.0)) f |= 2;
+    if (!(q[p + 4 * N] > 0.0)) f |= 4;
+  }
+  if (f) atomicOr(flag, f);
+}
+
+int check_state(cruna_ctx *c, const double *q) {
+  CRUNA_CUDA_CHECK(cudaMemsetAsync(c->flag, 0, sizeof(int), c->stream));
+  k_check<<<(int)std::min<long long>(nblocks(c->g.N), 148LL * 16), kThreads, 0, c->stream>>>(c->g.N, q,
+                                                                                             c->flag);
+  CRUNA_LAUNCH_CHECK(c);
+  int h = 0;
+  CRUNA_CUDA_CHECK(cudaMemcpyAsync(&h, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  return h;
+}
+
+// ------------------------------------------------------------------------------------------------
+// generic direct RHS: the call sequence of right_hand_side_direct_3d (ns_rho_rhou_p.f90:31-253)
+// with the point-wise work fused into a few kernels
+// ------------------------------------------------------------------------------------------------
+enum GenericField {
+  F_U1, F_U2, F_U3, F_T,
+  F_UX, F_UY, F_UZ, F_VX, F_VY, F_VZ, F_WX, F_WY, F_WZ, F_TX, F_TY, F_TZ,
+  F_MU, F_T11, F_T22, F_T33, F_T12, F_T13, F_T23, F_HX, F_HY, F_HZ,
+  // divergence terms
+  F_M1, F_M2, F_M3,                         // mass: d1(ru) d2(rv) d3(rw)
+  F_A1X, F_A1Y, F_A1Z, F_PX, F_V1X, F_V1Y, F_V1Z,
+  F_A2X, F_A2Y, F_A2Z, F_PY, F_V2X, F_V2Y, F_V2Z,
+  F_A3X, F_A3Y, F_A3Z, F_PZ, F_V3X, F_V3Y, F_V3Z,
+  F_EX, F_EY, F_EZ, F_QX, F_QY, F_QZ,
+  kGenericFields
+};
+
+__global__ void k_prim(long long N, const double *__restrict__ q, double *__restrict__ t, double WoR) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double r = q[p];
+    t[p + F_U1 * N] = q[p + N] / r;          // ns_rho_rhou_p.f90:95-99
+    t[p + F_U2 * N] = q[p + 2 * N] / r;
+    t[p + F_U3 * N] = q[p + 3 * N] / r;
+    t[p + F_T * N] = WoR * q[p + 4 * N] / r; // trafos.f90:57
+  }
+}
+
+// mu, tau, lambda*grad T (ns_rho_rhou_p.f90:115-128, 193-197)
+__global__ void k_visc(long long N, double *__restrict__ t, double mu0, double T0, double cp_over_pr) {
+  const double S1 = 110.4;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double T = t[p + F_T * N];
+    const double mu = mu0 * pow(T / T0, 1.5) * ((T0 + S1) / (T + S1));
+    const double ux = t[p + F_UX * N], uy = t[p + F_UY * N], uz = t[p + F_UZ * N];
+    const double vx = t[p + F_VX * N], vy = t[p + F_VY * N], vz = t[p + F_VZ * N];
+    const double wx = t[p + F_WX * N], wy = t[p + F_WY * N], wz = t[p + F_WZ * N];
+    const double mu_div = -(2.0 / 3.0 * mu * (ux + vy + wz));
+    t[p + F_MU * N] = mu;
+    t[p + F_T11 * N] = mu_div + 2 * mu * ux;
+    t[p + F_T22 * N] = mu_div + 2 * mu * vy;
+    t[p + F_T33 * N] = mu_div + 2 * mu * wz;
+    t[p + F_T12 * N] = mu * (uy + vx);
+    t[p + F_T13 * N] = mu * (uz + wx);
+    t[p + F_T23 * N] = mu * (vz + wy);
+    const double lam = mu * cp_over_pr;
+    t[p + F_HX * N] = lam * t[p + F_TX * N];
+    t[p + F_HY * N] = lam * t[p + F_TY * N];
+    t[p + F_HZ * N] = lam * t[p + F_TZ * N];
+  }
+}
+
+// assembly of the five equations in the reference's order (ns_rho_rhou_p.f90:131-209), + apply_force
+__global__ void k_assemble(long long N, const double *__restrict__ t, double *__restrict__ rhs,
+                           double gamma, const double *__restrict__ force) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+#define T_(f) t[p + (long long)(f) * N]
+    double r1 = -T_(F_M1) - T_(F_M2) - T_(F_M3);
+    double r2 = -T_(F_A1X) - T_(F_A1Y) - T_(F_A1Z) - T_(F_PX);
+    r2 = r2 + T_(F_V1X) + T_(F_V1Y) + T_(F_V1Z);
+    double r3 = -T_(F_A2X) - T_(F_A2Y) - T_(F_A2Z) - T_(F_PY);
+    r3 = r3 + T_(F_V2X) + T_(F_V2Y) + T_(F_V2Z);
+    double r4 = -T_(F_A3X) - T_(F_A3Y) - T_(F_A3Z) - T_(F_PZ);
+    r4 = r4 + T_(F_V3X) + T_(F_V3Y) + T_(F_V3Z);
+    const double gt = gamma / (gamma - 1.0);
+    double r5 = gt * (-T_(F_EX) - T_(F_EY) - T_(F_EZ));
+    r5 = r5 + T_(F_U1) * T_(F_PX) + T_(F_U2) * T_(F_PY) + T_(F_U3) * T_(F_PZ);
+    r5 = r5 + T_(F_QX) + T_(F_QY) + T_(F_QZ);
+    r5 = r5 + T_(F_T11) * T_(F_UX) + T_(F_T12) * T_(F_UY) + T_(F_T13) * T_(F_UZ) +
+         T_(F_T12) * T_(F_VX) + T_(F_T22) * T_(F_VY) + T_(F_T23) * T_(F_VZ) +
+         T_(F_T13) * T_(F_WX) + T_(F_T23) * T_(F_WY) + T_(F_T33) * T_(F_WZ);
+    r5 = (gamma - 1.0) * r5;
+#undef T_
+    if (force) {
+      r1 = r1 + force[p]; r2 = r2 + force[p + N]; r3 = r3 + force[p + 2 * N];
+      r4 = r4 + force[p + 3 * N]; r5 = r5 + force[p + 4 * N];
+    }
+    rhs[p] = r1; rhs[p + N] = r2; rhs[p + 2 * N] = r3; rhs[p + 3 * N] = r4; rhs[p + 4 * N] = r5;
+  }
+}
+
+void rhs_direct_generic(cruna_ctx *c, const double *q_in, double *rhs, double *qbc) {
+  const long long N = c->g.N;
+  double *t = c->tmp;
+  auto F = [&](int f) { return t + (long long)f * N; };
+  const double *q = q_in;
+  if (c->has_q_bc) {                                      // ns_rho_rhou_p.f90:89-92
+    copy_state(c, qbc, q_in, 5);
+    bc_q(c, qbc, 0);
+    q = qbc;
+  }
+  const double *ru = q + N, *rv = q + 2 * N, *rw = q + 3 * N, *pp = q + 4 * N;
+  const int blocks = (int)std::min<long long>(nblocks(N), 148LL * 32);
+  k_prim<<<blocks, kThreads, 0, c->stream>>>(N, q, t, c->cfg.W / c->cfg.R);
+  CRUNA_LAUNCH_CHECK(c);
+  const double *dx = c->dx;
+  // velocity gradients (:102-112)
+  for (int v = 0; v < 3; ++v)
+    for (int d = 0; d < 3; ++d) apply_diff(c, d, F(F_U1 + v), nullptr, F(F_UX + 3 * v + d), dx[d], 1);
+  // temperature gradient for the heat flux (:189-191), h absent unless heat_flux_dx
+  for (int d = 0; d < 3; ++d)
+    apply_diff(c, d, F(F_T), nullptr, F(F_TX + d), c->cfg.heat_flux_dx ? dx[d] : 1.0, 1);
+  k_visc<<<blocks, kThreads, 0, c->stream>>>(N, t, c->cfg.mu0, c->cfg.T0,
+                                             c->cfg.gamma * (c->cfg.R / c->cfg.W) / (c->cfg.gamma - 1.0) /
+                                                 c->cfg.Pr);
+  CRUNA_LAUNCH_CHECK(c);
+  // mass (:131-133)
+  apply_diff(c, 0, ru, nullptr, F(F_M1), dx[0], 1);
+  apply_diff(c, 1, rv, nullptr, F(F_M2), dx[1], 1);
+  apply_diff(c, 2, rw, nullptr, F(F_M3), dx[2], 1);
+  // momentum (:138-177): fluxes q(:,:,:,1+d)*u_v and the stress divergence
+  const int taus[3][3] = {{F_T11, F_T12, F_T13}, {F_T12, F_T22, F_T23}, {F_T13, F_T23, F_T33}};
+  const int afl[3][3] = {{F_A1X, F_A1Y, F_A1Z}, {F_A2X, F_A2Y, F_A2Z}, {F_A3X, F_A3Y, F_A3Z}};
+  const int vfl[3][3] = {{F_V1X, F_V1Y, F_V1Z}, {F_V2X, F_V2Y, F_V2Z}, {F_V3X, F_V3Y, F_V3Z}};
+  const double *rq[3] = {ru, rv, rw};
+  for (int v = 0; v < 3; ++v) {
+    for (int d = 0; d < 3; ++d) apply_diff(c, d, rq[d], F(F_U1 + v), F(afl[v][d]), dx[d], 1);
+    apply_diff(c, v, pp, nullptr, F(F_PX + 7 * v), dx[v], 1);
+    for (int d = 0; d < 3; ++d) apply_diff(c, d, F(taus[v][d]), nullptr, F(vfl[v][d]), dx[d], 1);
+  }
+  // pressure flux (:180-182) and heat flux divergence (:195-197)
+  for (int d = 0; d < 3; ++d) apply_diff(c, d, pp, F(F_U1 + d), F(F_EX + d), dx[d], 1);
+  for (int d = 0; d < 3; ++d)
+    apply_diff(c, d, F(F_HX + d), nullptr, F(F_QX + d), c->cfg.heat_flux_dx ? dx[d] : 1.0, 1);
+  k_assemble<<<blocks, kThreads, 0, c->stream>>>(N, t, rhs, c->cfg.gamma, c->force);
+  CRUNA_LAUNCH_CHECK(c);
+  if (c->has_rhs_bc) bc_rhs(c, rhs, q);                   // :218
+}
+
+// ------------------------------------------------------------------------------------------------
+// generic adjoint RHS: right_hand_side_adjoint_3d (ns_rho_rhou_p.f90:257-536)
+// ------------------------------------------------------------------------------------------------
+enum AdjField {
+  A_U1, A_U2, A_U3, A_GPR, A_IR,
+  A_D0, // 5 fields: D_d qs(v) for v = 0..4
+  A_S = A_D0 + 5,  // D_d(u_d * qs5)
+  A_P,             // D_d p
+  kAdjFields
+};
+
+__global__ void k_adj_prim(long long N, const double *__restrict__ q, double *__restrict__ t, double gamma) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double gm1 = gamma - 1.0;
+    t[p + A_GPR * N] = gamma * q[p + 4 * N] / (q[p] * gm1);   // :292-294
+    t[p + A_IR * N] = 1.0 / q[p];
+    t[p + A_U1 * N] = q[p + N] / q[p];                          // :299-301
+    t[p + A_U2 * N] = q[p + 2 * N] / q[p];
+    t[p + A_U3 * N] = q[p + 3 * N] / q[p];
+  }
+}
+
+// one direction's contribution (:317-370 for d=0, :386-440 for d=1, :456-509 for d=2)
+__global__ void k_adj_dir(long long N, int d, int first, const double *__restrict__ t,
+                          const double *__restrict__ qs, double *__restrict__ rhs, double gamma) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double gm1 = gamma - 1.0;
+    const double u1 = t[p + A_U1 * N], u2 = t[p + A_U2 * N], u3 = t[p + A_U3 * N];
+    const double gpr = t[p + A_GPR * N], ir = t[p + A_IR * N];
+    const double a = t[p + (A_D0 + 0) * N], b = t[p + (A_D0 + 1) * N], c = t[p + (A_D0 + 2) * N],
+                 dd = t[p + (A_D0 + 3) * N], e = t[p + (A_D0 + 4) * N];
+    const double sx = t[p + A_S * N], px = t[p + A_P * N];
+    const double qs5 = qs[p + 4 * N];
+    double r1 = first ? 0.0 : rhs[p], r2 = first ? 0.0 : rhs[p + N], r3 = first ? 0.0 : rhs[p + 2 * N],
+           r4 = first ? 0.0 : rhs[p + 3 * N], r5 = first ? 0.0 : rhs[p + 4 * N];
+    const double ud = d == 0 ? u1 : (d == 1 ? u2 : u3);
+    if (d == 0) {
+      r1 = r1 + (u1 * u1) * b + (u1 * u2) * c + (u1 * u3) * dd + gpr * u1 * e;
+      r2 = r2 - a - 2.0 * u1 * b - u2 * c - u3 * dd - gpr * e;
+      r3 = r3 - u1 * c;
+      r4 = r4 - u1 * dd;
+      r5 = r5 - gm1 * b - gamma * u1 * e;
+    } else if (d == 1) {
+      r1 = r1 + (u2 * u1) * b + (u2 * u2) * c + (u2 * u3) * dd + gpr * u2 * e;
+      r2 = r2 - u2 * b;
+      r3 = r3 - a - u1 * b - 2 * u2 * c - u3 * dd - gpr * e;
+      r4 = r4 - u2 * dd;
+      r5 = r5 - gm1 * c - gamma * u2 * e;
+    } else {
+      r1 = r1 + (u3 * u1) * b + (u3 * u2) * c + (u3 * u3) * dd + gpr * u3 * e;
+      r2 = r2 - u3 * b;
+      r3 = r3 - u3 * c;
+      r4 = r4 - a - u1 * b - u2 * c - 2 * u3 * dd - gpr * e;
+      r5 = r5 - gm1 * dd - gamma * u3 * e;
+    }
+    // -(A^T)^-1 (C^T qs)_d: D_d(-u_d*qs5) = -D_d(u_d*qs5)
+    r5 = r5 - gm1 * (-sx);
+    // +(A^T)^-1 C~_d p_d
+    r1 = r1 + qs5 * ud * ir * px;
+    if (d == 0) r2 = r2 - qs5 * ir * px;
+    else if (d == 1) r3 = r3 - qs5 * ir * px;
+    else r4 = r4 - qs5 * ir * px;
+    rhs[p] = r1; rhs[p + N] = r2; rhs[p + 2 * N] = r3; rhs[p + 3 * N] = r4; rhs[p + 4 * N] = r5;
+  }
+}
+
+void rhs_adjoint_generic(cruna_ctx *c, const double *qs_in, const double *q, const double *g, double *rhs,
+                         double *qsbc) {
+  const long long N = c->g.N;
+  double *t = c->tmp;
+  auto F = [&](int f) { return t + (long long)f * N; };
+  const double *qs = qs_in;
+  if (c->has_q_bc) {                                      // :287-290
+    copy_state(c, qsbc, qs_in, 5);
+    bc_qs(c, qsbc, q, 0);
+    qs = qsbc;
+  }
+  const int blocks = (int)std::min<long long>(nblocks(N), 148LL * 32);
+  k_adj_prim<<<blocks, kThreads, 0, c->stream>>>(N, q, t, c->cfg.gamma);
+  CRUNA_LAUNCH_CHECK(c);
+  for (int d = 0; d < 3; ++d) {
+    apply_diff(c, d, qs, nullptr, F(A_D0), c->dx[d], 5);                       // 5 fields at once
+    apply_diff(c, d, qs + 4 * N, F(A_U1 + d), F(A_S), c->dx[d], 1);            // D_d(u_d*qs5)
+    apply_diff(c, d, q + 4 * N, nullptr, F(A_P), c->dx[d], 1);                 // D_d p
+    k_adj_dir<<<blocks, kThreads, 0, c->stream>>>(N, d, d == 0, t, qs, rhs, c->cfg.gamma);
+    CRUNA_LAUNCH_CHECK(c);
+  }
+  if (g) add_fields(c, rhs, g, 5 * N);                                         // :512
+  if (c->has_rhs_bc) bc_rhss(c, rhs, qs, nullptr);                             // :518 (without q)
+}
+
+}  // namespace cruna
