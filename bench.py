@@ -1,0 +1,363 @@
+"""Benchmark of the CRUNA direct + adjoint time step on B200.
+
+Workload (the Taylor-Green configuration of the headline metric): 3-D Taylor-Green vortex, Mach 0.1,
+Re 1600, periodic [0, 2pi]^3 on 256^3 points, 8th-order explicit differences, 10th-order explicit
+filter (strength 0.2) in all three directions every step, classical RK4 at CFL 0.5, FP64.
+One "step" = one direct RK4 step (+ filters) followed by one adjoint RK4 step (+ filters) of the
+continuous adjoint on the direct state it produced; the unit is grid point-steps per second, i.e.
+points x (direct+adjoint step pairs) / s.  Inputs (q: 671 MB, qs: 671 MB) are larger than the 126 MB
+L2, so no explicit flush is needed between iterations.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 256]
+
+--impl reference times the CPU restatement of the reference's algorithm (the oracle; the Fortran
+reference itself cannot be built on this image) on all host cores with bounded samples.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "point-steps/s direct+adjoint"
+UNIT = "point-steps/s"
+
+# algorithmic HBM bytes per grid point and launch of each kernel family (FP64 state)
+ALG_BYTES_FP64 = {
+    "pass_g": 40 + 15 * 8,          # read q, write 15 fields
+    "pass_d": 9 * 8 + 6 * 8 + 140,  # read 9 stencil fields + 6 centre fields, RK stage I/O (average)
+    "adj_pass": 40 + 40 + 140,      # read qs, read frozen q, RK stage I/O (average)
+    "line_filter": 5 * 8 * 2,       # read + write 5 fields
+}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU legs (oracle): bounded samples of the same physics
+# ------------------------------------------------------------------------------------------------
+def _cpu_sample(n: int, pairs: int):
+    """Run `pairs` direct+adjoint step pairs of the oracle on an n^3 Taylor-Green sample; returns
+    (points*pairs, seconds)."""
+    import numpy as np
+
+    from oracle import cruna_oracle as O
+    from public_b200 import cases
+
+    s, q0 = cases.taylor_green(n=n, seed=0)
+    fields = {f.name for f in O.dataclasses.fields(O.Config)}
+    s["ai_freq"] = (1, 1, 1)
+    S = O.Solver(O.Config(**{k: v for k, v in s.items() if k in fields}))
+    qs = np.asfortranarray(1e-3 * np.ones_like(q0))
+    q = q0
+    t0 = time.perf_counter()
+    for it in range(pairs):
+        q = S.calc_direct(q, 1, nt0=it)
+        qs, _ = S.calc_adjoint(qs, [q, q])
+    dt = time.perf_counter() - t0
+    return n ** 3 * pairs, dt
+
+
+def cpu_baseline(cores: int, n: int = 64, pairs: int = 2):
+    """Oracle timed on `cores` host processes (spawned, one independent sample each)."""
+    if cores <= 1:
+        pts, dt = _cpu_sample(n, pairs)
+        return pts / dt, dt
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        res = pool.starmap(_cpu_sample, [(n, pairs)] * cores)
+    wall = time.perf_counter() - t0
+    pts = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    return pts / busy, wall
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    n = args.ref_n
+    # every timed step is one direct+adjoint pair on an n^3 sample per core
+    for _ in range(args.warmup):
+        pass
+    t0 = time.perf_counter()
+    vals = []
+    for _ in range(max(1, args.steps)):
+        v, _ = cpu_baseline(cores, n=n, pairs=1)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    value = statistics.median(vals)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Taylor-Green state)",
+        "config": {"workload": f"taylor-green {args.n}^3, o8 FD + o10 filter, RK4, direct+adjoint step",
+                   "sample": f"{n}^3 Taylor-Green per core, 1 step pair per timed step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{cores} x {n}^3 Taylor-Green, one direct+adjoint pair each"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "numpy restatement of the reference algorithm (Fortran/MPI/HDF5 build unavailable here)",
+    }
+    print(json.dumps(out))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+
+    # CPU baseline first (spawned processes, before heavy GPU work), rank 0 at N=1 only
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, wall = cpu_baseline(1, n=48, pairs=2)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "48^3 Taylor-Green, 2 direct+adjoint step pairs, numpy oracle on 1 core",
+               "seconds": round(wall, 2)}
+
+    from public_b200 import cases
+    from public_b200.cruna import Cruna, Settings
+
+    s, q0 = cases.taylor_green(n=args.n, seed=rank)
+    s["ai_freq"] = (1, 1, 1)
+    st = Settings.from_dict(s)
+    st.device = local
+    st.precision = args.precision
+    ctx = Cruna(st)
+    N = args.n ** 3
+    dev = torch.device("cuda", local)
+    q = torch.from_numpy(np.ascontiguousarray(q0.ravel(order="F"))).to(dev)
+    qs = torch.full_like(q, 1e-3)
+    qp, qsp = q.data_ptr(), qs.data_ptr()
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+    torch.cuda.synchronize()
+
+    def step(nt):
+        ctx.run_direct_dev(qp, nt, 1)
+        ctx.run_adjoint_dev(qsp, qp, None, nt + 1, 1)
+
+    for w in range(args.warmup):
+        step(w)
+    ctx.sync()
+
+    # ---- device-resident timing -----------------------------------------------------------------
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    ctx.profile(True)
+    launches0 = ctx.launches
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        nt = args.warmup + k
+        ev[k][0].record(stream)
+        ctx.run_direct_dev(qp, nt, 1)
+        ev[k][1].record(stream)
+        ctx.run_adjoint_dev(qsp, qp, None, nt + 1, 1)
+        ev[k][2].record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = ctx.launches - launches0
+    prof = ctx.profile_report()
+    ctx.profile(False)
+    t_dir = sum(e[0].elapsed_time(e[1]) for e in ev)
+    t_adj = sum(e[1].elapsed_time(e[2]) for e in ev)
+    t_tot = sum(e[0].elapsed_time(e[2]) for e in ev)
+    if dist:
+        t = torch.tensor([t_tot, t_dir, t_adj], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_tot, t_dir, t_adj = [float(x) for x in t.tolist()]
+    ms = t_tot / args.steps
+    value = world * N * args.steps / (t_tot / 1e3)
+
+    # ---- end-to-end through the host-pointer C ABI (pinned host buffers) ------------------------
+    hq = torch.empty(5 * N, dtype=torch.float64, pin_memory=True)
+    hqs = torch.empty(5 * N, dtype=torch.float64, pin_memory=True)
+    hq.copy_(q.cpu())
+    hqs.copy_(qs.cpu())
+    import ctypes as C
+    lib = ctx.lib
+    e2e_steps = max(1, min(args.steps, 3))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        nt = args.warmup + args.steps + k
+        ctx._check(lib.cruna_run_direct(ctx.h, C.c_void_p(hq.data_ptr()), nt, 1, None))
+        ctx._check(lib.cruna_run_adjoint(ctx.h, C.c_void_p(hqs.data_ptr()), C.c_void_p(hq.data_ptr()), None,
+                                         nt + 1, 1))
+    t_e2e = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([t_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e_value = world * N * e2e_steps / t_e2e
+    bytes_state = 5 * N * 8
+
+    # ---- roofline of the dominant kernel --------------------------------------------------------
+    peak, peak_kind = load_peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    roof = None
+    if dom:
+        name, (cnt, tot_ms) = dom
+        per_pt = ALG_BYTES_FP64.get(name)
+        if per_pt is not None and args.precision == "fp32" and name == "pass_g":
+            per_pt = 40 + 15 * 4
+        if per_pt is not None and args.precision == "fp32" and name == "pass_d":
+            per_pt = 15 * 4 + 140
+        avg_s = tot_ms / cnt / 1e3
+        achieved = (per_pt * N / avg_s / 1e9) if per_pt else None
+        roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "traffic": traffic_from_profiles(name, args.n, args.precision),
+                "alg_bytes_per_point": per_pt, "avg_launch_ms": avg_s * 1e3, "launches": cnt}
+    kernels = {k: {"launches": v[0], "total_ms": round(v[1], 3), "share": round(v[1] / max(t_tot, 1e-9), 4)}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+    B_alg = 760 + 920
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-stencil/f64-state",
+        "data": "synthetic (seeded Taylor-Green state, 1e-4 density noise)",
+        "config": {"workload": f"taylor-green {args.n}^3 Mach 0.1 Re 1600: o8 FD, o10 explicit filter every "
+                               f"step, RK4 direct step + continuous-adjoint RK4 step",
+                   "points": N, "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "inputs (671 MB per state) larger than L2; no flush",
+                   "precision": args.precision, "rhs_path": ctx.rhs_path},
+        "direct": {"value": N * args.steps / (t_dir / 1e3), "unit": UNIT, "ms_per_step": t_dir / args.steps},
+        "adjoint": {"value": N * args.steps / (t_adj / 1e3), "unit": UNIT, "ms_per_step": t_adj / args.steps},
+        "hbm_alg": {"bytes_per_point_step": B_alg, "achieved_gbs": value / world * B_alg / 1e9,
+                    "frac": value / world * B_alg / 1e9 / peak},
+        "roofline": roof,
+        "kernels": kernels,
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * bytes_state,
+                "d2h_bytes_per_step": 2 * bytes_state, "steps": e2e_steps,
+                "api": "cruna_run_direct + cruna_run_adjoint on pinned host buffers"},
+        "cpu_baseline": cpu,
+    }
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
+def traffic_from_profiles(kernel: str, n: int, precision: str):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary, scaled to n^3 points."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_tgv_{precision}.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_point:"):
+                    return float(line.split(":")[1]) * n ** 3
+    except OSError:
+        pass
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--ref-n", type=int, default=48)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -207,6 +207,12 @@ int cruna_set_force_generic(cruna_ctx *ctx, int force_generic);
 /* Number of kernels this library enqueued since the context was created (for launch accounting). */
 int64_t cruna_kernel_launches(const cruna_ctx *ctx);
 
+/* Kernel timing: while enabled, each kernel family (fused passes, filters, stage updates, generic
+   line operators) is bracketed by CUDA events on the context's stream.  cruna_profile_report drains
+   them and writes lines "name launches total_ms" into buf; it returns the length of the full report. */
+int cruna_profile_enable(cruna_ctx *ctx, int on);
+int cruna_profile_report(cruna_ctx *ctx, char *buf, int buflen);
+
 /* The library's restatement of LAPACK dgttrf / dgttrs('N', nrhs=1), which every compact core of the
    reference calls (e.g. diff_pen_core_o6_i_c_p.f90:135,213,219); exported so callers and tests can
    compare its factors with their LAPACK.  ipiv is 1-based as in LAPACK. */

@@ -106,6 +106,8 @@ _SIGNATURES = {
     "cruna_rhs_path": (_I, [_P]),
     "cruna_set_force_generic": (_I, [_P, _I]),
     "cruna_kernel_launches": (C.c_int64, [_P]),
+    "cruna_profile_enable": (_I, [_P, _I]),
+    "cruna_profile_report": (_I, [_P, C.c_char_p, _I]),
     "cruna_lapack_dgttrf": (_I, [_I, _P, _P, _P, _P, _P]),
     "cruna_lapack_dgttrs": (None, [_I, _P, _P, _P, _P, _P, _P]),
 }
@@ -406,6 +408,22 @@ class Cruna:
         self._check(self.lib.cruna_run_adjoint_dev(self.h, C.c_void_p(qs_ptr), C.c_void_p(Q_ptr),
                                                    None if g_ptr is None else C.c_void_p(g_ptr),
                                                    int(nt_end), int(nsteps)))
+
+    def profile(self, on: bool = True):
+        self._check(self.lib.cruna_profile_enable(self.h, 1 if on else 0))
+
+    def profile_report(self) -> dict:
+        """{kernel family: (launches, total ms)} since profiling was enabled."""
+        n = self.lib.cruna_profile_report(self.h, None, 0)
+        if n < 0:
+            self._check(n)
+        buf = C.create_string_buffer(n + 1)
+        self.lib.cruna_profile_report(self.h, buf, n + 1)
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, cnt, ms = line.split()
+            out[name] = (int(cnt), float(ms))
+        return out
 
     def sync(self):
         self._check(self.lib.cruna_sync(self.h))

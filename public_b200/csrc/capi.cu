@@ -125,6 +125,13 @@ void step_direct(cruna_ctx *c, const double *q0, double *q1) {
 void step_adjoint(cruna_ctx *c, const double *qs0, const double *q0, const double *g, double *qs1) {
   double *k = c->st[0], *acc = c->st[1], *qa = c->st[2], *qb = c->st[3], *qbc = c->st[4];
   const double dt = -c->cfg.dt;
+  if (use_fused(c)) {
+    rhs_adjoint_fused(c, qs0, q0, g, k, 1, qs0, acc, qa, dt);
+    rhs_adjoint_fused(c, qa, q0, g, k, 2, qs0, acc, qb, dt);
+    rhs_adjoint_fused(c, qb, q0, g, k, 3, qs0, acc, qa, dt);
+    rhs_adjoint_fused(c, qa, q0, g, k, 4, qs0, acc, qs1, dt);
+    return;
+  }
   ensure_generic(c);
   rhs_adjoint_generic(c, qs0, q0, g, k, qbc);
   rk_stage(c, 1, dt, k, qs0, acc, qa);
@@ -155,6 +162,52 @@ int dir_index(cruna_ctx *c, int dir) {
 }
 
 }  // namespace
+
+namespace cruna {
+
+int prof_begin(cruna_ctx *c, const char *name) {
+  if (!c->prof_on) return -1;
+  auto take = [&]() {
+    cudaEvent_t e;
+    if (!c->prof_pool.empty()) {
+      e = c->prof_pool.back();
+      c->prof_pool.pop_back();
+    } else {
+      CRUNA_CUDA_CHECK(cudaEventCreate(&e));
+    }
+    return e;
+  };
+  if (c->prof_pending.size() >= 4096) prof_drain(c);
+  cudaEvent_t a = take(), b = take();
+  CRUNA_CUDA_CHECK(cudaEventRecord(a, c->stream));
+  c->prof_pending.push_back({name, a, b});
+  return (int)c->prof_pending.size() - 1;
+}
+
+void prof_end(cruna_ctx *c, int idx) {
+  if (idx < 0 || idx >= (int)c->prof_pending.size()) return;
+  cudaEventRecord(c->prof_pending[idx].b, c->stream);
+}
+
+void prof_drain(cruna_ctx *c) {
+  if (c->prof_pending.empty()) return;
+  CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  for (auto &e : c->prof_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+      auto &acc = c->prof_acc[e.name];
+      acc.first += 1;
+      acc.second += ms;
+    } else {
+      cudaGetLastError();
+    }
+    c->prof_pool.push_back(e.a);
+    c->prof_pool.push_back(e.b);
+  }
+  c->prof_pending.clear();
+}
+
+}  // namespace cruna
 
 extern "C" {
 
@@ -346,6 +399,7 @@ int cruna_init(const cruna_config *cfg, const double *bc_table, int nbc, cruna_c
     c->allocations.push_back(fl);
     c->flag = static_cast<int *>(fl);
     c->fused_ok = fused_supported(c);
+    c->filter_fused_ok = filter_fused_supported(c);
     CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
     return CRUNA_OK;
   });
@@ -358,10 +412,38 @@ int cruna_init(const cruna_config *cfg, const double *bc_table, int nbc, cruna_c
   return CRUNA_OK;
 }
 
+int cruna_profile_enable(cruna_ctx *c, int on) {
+  return guarded(c, [&]() -> int {
+    if (!on) prof_drain(c);
+    c->prof_on = on != 0;
+    if (on) c->prof_acc.clear();
+    return CRUNA_OK;
+  });
+}
+
+int cruna_profile_report(cruna_ctx *c, char *buf, int buflen) {
+  return guarded(c, [&]() -> int {
+    prof_drain(c);
+    std::string out;
+    for (auto &kv : c->prof_acc)
+      out += kv.first + " " + std::to_string(kv.second.first) + " " + std::to_string(kv.second.second) + "\n";
+    if (buf && buflen > 0) {
+      std::strncpy(buf, out.c_str(), (size_t)buflen - 1);
+      buf[buflen - 1] = 0;
+    }
+    return (int)out.size();
+  });
+}
+
 void cruna_free(cruna_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto &e : c->prof_pending) {
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+  for (auto e : c->prof_pool) cudaEventDestroy(e);
   for (void *p : c->allocations) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -509,8 +591,12 @@ int cruna_rhs_adjoint_dev(cruna_ctx *c, const double *qs, const double *q, const
                           double /*t*/) {
   return guarded(c, [&]() -> int {
     if (!qs || !q || !rhs) fail(c, CRUNA_ERR_ARG, "null pointer");
-    ensure_generic(c);
-    rhs_adjoint_generic(c, qs, q, g, rhs, c->st[4]);
+    if (use_fused(c)) {
+      rhs_adjoint_fused(c, qs, q, g, rhs, 0, nullptr, nullptr, nullptr, 0.0);
+    } else {
+      ensure_generic(c);
+      rhs_adjoint_generic(c, qs, q, g, rhs, c->st[4]);
+    }
     return CRUNA_OK;
   });
 }
@@ -654,10 +740,17 @@ int cruna_check_state_dev(cruna_ctx *c, const double *q) {
 static int run_direct_impl(cruna_ctx *c, double *q, int nt0, int nsteps, double *traj, bool traj_host) {
   for (int s = 1; s <= nsteps; ++s) {
     const int nt = nt0 + s;
-    step_direct(c, q, q);
-    if (c->has_q_bc) bc_q(c, q, 1);                               // :82
-    for (int d = 0; d < 3; ++d)
-      if (due(c->cfg.di_freq[d], nt)) apply_filter(c, d, q, c->st[5], 5);   // :85-95
+    const int on[3] = {due(c->cfg.di_freq[0], nt), due(c->cfg.di_freq[1], nt), due(c->cfg.di_freq[2], nt)};
+    if (c->filter_fused_ok && !c->force_generic && (on[0] || on[1] || on[2])) {
+      step_direct(c, q, c->st[5]);
+      if (c->has_q_bc) bc_q(c, c->st[5], 1);                      // :82
+      filter3_fused(c, c->st[5], q, on);                          // :85-95
+    } else {
+      step_direct(c, q, q);
+      if (c->has_q_bc) bc_q(c, q, 1);                             // :82
+      for (int d = 0; d < 3; ++d)
+        if (on[d]) apply_filter(c, d, q, c->st[5], 5);            // :85-95
+    }
     if (traj) {                                                    // :98-100
       double *dst = traj + (long long)(s - 1) * N5(c);
       CRUNA_CUDA_CHECK(cudaMemcpyAsync(dst, q, sizeof(double) * N5(c),
@@ -700,10 +793,17 @@ static int run_adjoint_impl(cruna_ctx *c, double *qs, const double *Q, const dou
       q0 = dq;
       g = G ? stage_in(c, 2, G + off, 5) : nullptr;
     }
-    step_adjoint(c, qs, q0, g, qs);                               // :81
-    if (c->has_q_bc) bc_qs(c, qs, q0, 1);                          // :88
-    for (int d = 0; d < 3; ++d)
-      if (due(c->cfg.ai_freq[d], nt)) apply_filter(c, d, qs, c->st[5], 5);   // :91-101
+    const int on[3] = {due(c->cfg.ai_freq[0], nt), due(c->cfg.ai_freq[1], nt), due(c->cfg.ai_freq[2], nt)};
+    if (c->filter_fused_ok && !c->force_generic && (on[0] || on[1] || on[2])) {
+      step_adjoint(c, qs, q0, g, c->st[5]);                       // :81
+      if (c->has_q_bc) bc_qs(c, c->st[5], q0, 1);                  // :88
+      filter3_fused(c, c->st[5], qs, on);                          // :91-101
+    } else {
+      step_adjoint(c, qs, q0, g, qs);                             // :81
+      if (c->has_q_bc) bc_qs(c, qs, q0, 1);                        // :88
+      for (int d = 0; d < 3; ++d)
+        if (on[d]) apply_filter(c, d, qs, c->st[5], 5);           // :91-101
+    }
     if (c->cfg.check_every > 0 && nt % c->cfg.check_every == 0) {
       int f = check_state(c, qs);
       if (f & 1) fail(c, CRUNA_ERR_STATE, "adjoint state not finite at step " + std::to_string(nt));

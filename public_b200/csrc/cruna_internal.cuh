@@ -4,7 +4,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/cruna_b200.h"
@@ -96,6 +99,19 @@ struct cruna_ctx {
   std::string err;
   bool force_generic = false;
   bool fused_ok = false;
+  bool filter_fused_ok = false;
+  // FP32-stencil path: pressure / temperature offsets differenced in FP32 (set once per context)
+  bool refs_set = false;
+  double p_ref = 0.0, T_ref = 0.0;
+  // kernel timing (cruna_profile_enable): events bracketing launches on the context's stream
+  bool prof_on = false;
+  struct ProfEntry {
+    const char *name;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfEntry> prof_pending;
+  std::vector<cudaEvent_t> prof_pool;
+  std::map<std::string, std::pair<long long, double>> prof_acc;
   // device memory
   std::vector<void *> allocations;
   double *qref = nullptr;        // 5N
@@ -126,6 +142,10 @@ void rhs_adjoint_generic(cruna_ctx *c, const double *qs, const double *q, const 
 bool fused_supported(const cruna_ctx *c);
 void rhs_direct_fused(cruna_ctx *c, const double *q, double *rhs, int stage, const double *q0,
                       double *acc, double *qnext, double dt);
+void rhs_adjoint_fused(cruna_ctx *c, const double *qs, const double *q, const double *g, double *rhs,
+                       int stage, const double *qs0, double *acc, double *qnext, double dt);
+bool filter_fused_supported(const cruna_ctx *c);
+void filter3_fused(cruna_ctx *c, const double *in, double *out, const int on[3]);
 void bc_q(cruna_ctx *c, double *q, int outside);
 void bc_qs(cruna_ctx *c, double *qs, const double *q, int outside);
 void bc_rhs(cruna_ctx *c, double *rhs, const double *q);
@@ -135,6 +155,17 @@ void rk_stage(cruna_ctx *c, int stage, double dt, const double *k, const double 
 void copy_state(cruna_ctx *c, double *dst, const double *src, int nfields);
 int check_state(cruna_ctx *c, const double *q);
 void add_fields(cruna_ctx *c, double *dst, const double *src, long long n);
+
+// kernel timing helpers (capi.cu)
+int prof_begin(cruna_ctx *c, const char *name);
+void prof_end(cruna_ctx *c, int idx);
+void prof_drain(cruna_ctx *c);
+struct ProfScope {
+  cruna_ctx *c;
+  int idx;
+  ProfScope(cruna_ctx *ctx, const char *name) : c(ctx), idx(prof_begin(ctx, name)) {}
+  ~ProfScope() { prof_end(c, idx); }
+};
 
 }  // namespace cruna
 

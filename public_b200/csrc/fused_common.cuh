@@ -1,0 +1,181 @@
+// Shared pieces of the fused z-marching kernels: the explicit line operator in compact form and
+// the derivative evaluators on shared-memory rows (x, y) and register columns (z).
+#pragma once
+
+#include "cruna_internal.cuh"
+
+namespace cruna {
+namespace fz {
+
+constexpr int TX = 32;
+constexpr int TY = 4;
+constexpr int NG = 15;   // pass-G outputs per point
+
+// compact description of an explicit line operator for the fused kernels
+struct DirOpF {
+  int n = 1, kind = 0, periodic = 0, r = 0, nb = 0, bw = 0;
+  double c[5] = {0};
+  double brow[2][5] = {{0}};
+  double scale = 0.0;    // 1/(dx*div)
+  double scale_h = 0.0;  // heat-flux derivatives: 1/div (reference, h absent) or 1/(dx*div)
+};
+
+struct FusedArgs {
+  Grid g;
+  DirOpF op[3];
+  int kc;                       // z-chunk length of one block
+  // material (ns_rho_rhou_p_trafos.f90)
+  double WoR, mu0, T0, cp_over_pr, gamma;
+  double p_ref, T_ref;          // FP32 path offsets (0 in the FP64 path)
+  // pass G
+  const double *q;
+  void *gbuf;                   // NG fields of T
+  // pass D
+  double *rhs;
+  const double *force;
+  int stage;                    // 0: write rhs; 1..4: RK4 stage update
+  double dt;
+  const double *q0;
+  double *acc;
+  double *qnext;
+};
+
+__host__ __device__ constexpr int ring_slots(int R) { return 2 * R + 1; }
+
+template <typename T, int R>
+__device__ __forceinline__ T dsm(const DirOpF &op, const T *p, int s, int i) {
+  // derivative (unscaled) at line position i; p points at the point, neighbours at p[m*s]
+  if (op.kind == 0) return T(0);
+  if (op.periodic || (i >= op.nb && i < op.n - op.nb)) {
+    T t = T(op.c[1]) * (p[s] - p[-s]);
+#pragma unroll
+    for (int m = 2; m <= R; ++m)
+      if (m <= op.r) t = t + T(op.c[m]) * (p[m * s] - p[-m * s]);
+    return t;
+  }
+  const bool start = i < op.nb;
+  const int row = start ? i : op.n - 1 - i;
+  T t = T(0);
+  for (int m = 0; m < op.bw; ++m) {
+    const int j = start ? m : op.n - 1 - m;
+    const T v = p[(j - i) * s];
+    t = (m == 0) ? T(op.brow[row][0]) * v : t + T(op.brow[row][m]) * v;
+  }
+  return start ? t : -t;
+}
+
+// derivative of a product a*b
+template <typename T, int R>
+__device__ __forceinline__ T dsm2(const DirOpF &op, const T *a, const T *b, int s, int i) {
+  if (op.kind == 0) return T(0);
+  if (op.periodic || (i >= op.nb && i < op.n - op.nb)) {
+    T t = T(op.c[1]) * (a[s] * b[s] - a[-s] * b[-s]);
+#pragma unroll
+    for (int m = 2; m <= R; ++m)
+      if (m <= op.r) t = t + T(op.c[m]) * (a[m * s] * b[m * s] - a[-m * s] * b[-m * s]);
+    return t;
+  }
+  const bool start = i < op.nb;
+  const int row = start ? i : op.n - 1 - i;
+  T t = T(0);
+  for (int m = 0; m < op.bw; ++m) {
+    const int j = start ? m : op.n - 1 - m;
+    const T v = a[(j - i) * s] * b[(j - i) * s];
+    t = (m == 0) ? T(op.brow[row][0]) * v : t + T(op.brow[row][m]) * v;
+  }
+  return start ? t : -t;
+}
+
+// z-derivatives from a register column v[0..2R] centred at v[R]: the closure rows are evaluated with
+// compile-time offsets only, so the column stays in registers
+template <typename T, int R>
+__device__ __forceinline__ T dsz(const DirOpF &op, const T *v, int k) {
+  if (op.kind == 0) return T(0);
+  if (op.periodic || (k >= op.nb && k < op.n - op.nb)) {
+    T t = T(op.c[1]) * (v[R + 1] - v[R - 1]);
+#pragma unroll
+    for (int m = 2; m <= R; ++m)
+      if (m <= op.r) t = t + T(op.c[m]) * (v[R + m] - v[R - m]);
+    return t;
+  }
+  const bool start = k < op.nb;
+  const int row = start ? k : op.n - 1 - k;
+  T t = T(0);
+  bool first = true;
+  if (start) {
+#pragma unroll
+    for (int o = -R; o <= R; ++o) {
+      const int j = k + o;
+      if (j >= 0 && j < op.bw) {
+        const T c = T(op.brow[row][j]);
+        t = first ? c * v[R + o] : t + c * v[R + o];
+        first = false;
+      }
+    }
+    return t;
+  }
+#pragma unroll
+  for (int o = R; o >= -R; --o) {
+    const int m = op.n - 1 - (k + o);
+    if (m >= 0 && m < op.bw) {
+      const T c = T(op.brow[row][m]);
+      t = first ? c * v[R + o] : t + c * v[R + o];
+      first = false;
+    }
+  }
+  return -t;
+}
+
+template <typename T, int R>
+__device__ __forceinline__ T dsz2(const DirOpF &op, const T *a, const T *b, int k) {
+  if (op.kind == 0) return T(0);
+  if (op.periodic || (k >= op.nb && k < op.n - op.nb)) {
+    T t = T(op.c[1]) * (a[R + 1] * b[R + 1] - a[R - 1] * b[R - 1]);
+#pragma unroll
+    for (int m = 2; m <= R; ++m)
+      if (m <= op.r) t = t + T(op.c[m]) * (a[R + m] * b[R + m] - a[R - m] * b[R - m]);
+    return t;
+  }
+  const bool start = k < op.nb;
+  const int row = start ? k : op.n - 1 - k;
+  T t = T(0);
+  bool first = true;
+  if (start) {
+#pragma unroll
+    for (int o = -R; o <= R; ++o) {
+      const int j = k + o;
+      if (j >= 0 && j < op.bw) {
+        const T c = T(op.brow[row][j]);
+        const T v = a[R + o] * b[R + o];
+        t = first ? c * v : t + c * v;
+        first = false;
+      }
+    }
+    return t;
+  }
+#pragma unroll
+  for (int o = R; o >= -R; --o) {
+    const int m = op.n - 1 - (k + o);
+    if (m >= 0 && m < op.bw) {
+      const T c = T(op.brow[row][m]);
+      const T v = a[R + o] * b[R + o];
+      t = first ? c * v : t + c * v;
+      first = false;
+    }
+  }
+  return -t;
+}
+
+// global index along a direction for a cell offset; -1 when outside an open line
+__device__ __forceinline__ int gidx(const DirOpF &op, int g) {
+  if (g >= 0 && g < op.n) return g;
+  if (op.periodic) return ((g % op.n) + op.n) % op.n;
+  return -1;
+}
+
+
+DirOpF to_dir(const LineOp &op, double dx, bool heat_dx);
+int halo_of(const LineOp &op);
+
+}  // namespace fz
+}  // namespace cruna

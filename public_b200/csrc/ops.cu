@@ -151,12 +151,14 @@ void launch_line_stencil(cruna_ctx *c, const LineOp &op, int dir, const double *
                          double *out, double scale, int nfields, double sign) {
   const long long work = c->g.N * nfields;
   const int blocks = (int)std::min<long long>(nblocks(work), 148LL * 64);
+  ProfScope ps(c, op.antisym ? "line_diff" : "line_filter");
   k_line_stencil<<<blocks, kThreads, 0, c->stream>>>(op, c->g, dir, f1, f2, out, scale, sign, nfields);
   CRUNA_LAUNCH_CHECK(c);
 }
 
 void launch_line_solve(cruna_ctx *c, const LineOp &op, int dir, double *data, int nfields) {
   const long long lines = (c->g.N / op.n) * nfields;
+  ProfScope ps(c, "line_solve");
   k_line_solve<<<nblocks(lines, 128), 128, 0, c->stream>>>(op, c->g, dir, data, nfields);
   CRUNA_LAUNCH_CHECK(c);
 }
@@ -490,6 +492,7 @@ __global__ void k_rk_stage(int stage, long long M, double dt, const double *__re
 void rk_stage(cruna_ctx *c, int stage, double dt, const double *k, const double *q0, double *acc,
               double *qnext) {
   const long long M = c->g.N * 5;
+  ProfScope ps(c, "rk_stage");
   k_rk_stage<<<(int)std::min<long long>(nblocks(M), 148LL * 32), kThreads, 0, c->stream>>>(stage, M, dt, k,
                                                                                            q0, acc, qnext);
   CRUNA_LAUNCH_CHECK(c);
