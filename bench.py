@@ -37,6 +37,8 @@ ALG_BYTES_FP64 = {
     "pass_d": 9 * 8 + 6 * 8 + 140,  # read 9 stencil fields + 6 centre fields, RK stage I/O (average)
     "adj_pass": 40 + 40 + 140,      # read qs, read frozen q, RK stage I/O (average)
     "line_filter": 5 * 8 * 2,       # read + write 5 fields
+    "filter_xy": 5 * 8 * 2,         # read + write 5 fields (x and y filters of each plane)
+    "filter_z": 5 * 8 * 2,          # read + write 5 fields
 }
 
 

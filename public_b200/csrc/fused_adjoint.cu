@@ -71,12 +71,12 @@ __device__ __forceinline__ void adj_dir(int d, double u1, double u2, double u3, 
 }
 
 // plane fields: 0..4 qs1..qs5, 5 p, 6 u, 7 v ; column fields: 0..4 qs1..qs5, 5 p, 6 w
-template <int R>
+template <int R, bool PER>
 __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ AdjArgs a) {
   using T = double;
   constexpr int PW = TX + 2 * R, PH = TY + 2 * R, PS = PW * PH;
   constexpr int NS = ring_slots(R);
-  constexpr int NPF = 8, NRF = 7;
+  constexpr int NPF = 8, NRF = 7, RS = TX * TY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *plane = reinterpret_cast<T *>(smem_raw);          // [NPF][PH][PW]
   T *ring = plane + NPF * PS;                          // [NS][NRF][TY*TX]
@@ -85,160 +85,170 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
   const int k0 = blockIdx.z * a.kc;
   const int k1 = min(k0 + a.kc, a.g.n3);
   const DirOpF &ox = a.op[0], &oy = a.op[1], &oz = a.op[2];
+  const int n1 = a.g.n1, n12 = a.g.n1 * a.g.n2;
   const int gi = gidx(ox, i0 + tx), gj = gidx(oy, j0 + ty);
-  const long long N = a.g.N, n1 = a.g.n1, n12 = (long long)a.g.n1 * a.g.n2;
+  const long long N = a.g.N;
   const bool inside = (i0 + tx) < a.g.n1 && (j0 + ty) < a.g.n2;
   const bool col = gi >= 0 && gj >= 0;
-  const long long colpt = gi + n1 * gj;
+  const int colpt = gi + n1 * gj;
+  const double *S0 = a.qs, *S1 = a.qs + N, *S2 = a.qs + 2 * N, *S3 = a.qs + 3 * N, *S4 = a.qs + 4 * N;
+  const double *Q0 = a.q, *Q1 = a.q + N, *Q2 = a.q + 2 * N, *Q3 = a.q + 3 * N, *Q4 = a.q + 4 * N;
+  HaloSet<R> hs;
+  hs.init(ox, oy, i0, j0, tid, n1);
 
-  auto ring_at = [&](int slot, int f) -> T * { return ring + (slot * NRF + f) * (TX * TY) + tid; };
-  auto put_ring = [&](int kk, const double *qsv, double rho, double rw, double p) {
-    const int sl = ((kk % NS) + NS) % NS;
+  auto put_ring = [&](int kk, const double *v8) {
+    // v8: qs1..qs5, rho, rho*w, p
+    T *rp = ring + (((kk % NS) + NS) % NS) * NRF * RS + tid;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) *ring_at(sl, v) = qsv[v];
-    *ring_at(sl, 5) = p;
-    *ring_at(sl, 6) = rw * (1.0 / rho);
+    for (int f = 0; f < 5; ++f) rp[f * RS] = v8[f];
+    rp[5 * RS] = v8[7];
+    rp[6 * RS] = v8[6] * (1.0 / v8[5]);
+  };
+  auto load8 = [&](long long pt, double *v8) {
+    v8[0] = S0[pt]; v8[1] = S1[pt]; v8[2] = S2[pt]; v8[3] = S3[pt]; v8[4] = S4[pt];
+    v8[5] = Q0[pt]; v8[6] = Q3[pt]; v8[7] = Q4[pt];
   };
   for (int kk = k0 - R; kk < k0 + R; ++kk) {
     const int gk = gidx(oz, kk);
     if (gk < 0 || !col) continue;
-    const long long pt = colpt + n12 * gk;
-    double qsv[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) qsv[v] = a.qs[pt + v * N];
-    put_ring(kk, qsv, a.q[pt], a.q[pt + 3 * N], a.q[pt + 4 * N]);
+    double v8[8];
+    load8(colpt + (long long)n12 * gk, v8);
+    put_ring(kk, v8);
   }
-  // register prefetch: ring plane k+R (qs 5 + rho, rho*w, p) and centre rho, rho*u, rho*v of plane k
+  // register prefetch of the ring plane k+R+1 and the centre (rho, rho*u, rho*v) of plane k+1
   double pf[8];
   double pc[3] = {1.0, 0.0, 0.0};
-  int pf_k = -1;
+  int pf_ok = 0;
   auto prefetch = [&](int kk, int kc) {
     const int gk = gidx(oz, kk);
-    pf_k = (gk >= 0 && col) ? gk : -1;
-    if (pf_k >= 0) {
-      const long long pt = colpt + n12 * gk;
-#pragma unroll
-      for (int v = 0; v < 5; ++v) pf[v] = a.qs[pt + v * N];
-      pf[5] = a.q[pt];
-      pf[6] = a.q[pt + 3 * N];
-      pf[7] = a.q[pt + 4 * N];
-    }
+    pf_ok = (gk >= 0 && col);
+    if (pf_ok) load8(colpt + (long long)n12 * gk, pf);
     if (col && kc < k1) {
-      const long long pt = colpt + n12 * kc;
-      pc[0] = a.q[pt];
-      pc[1] = a.q[pt + N];
-      pc[2] = a.q[pt + 2 * N];
+      const long long pt = colpt + (long long)n12 * kc;
+      pc[0] = Q0[pt];
+      pc[1] = Q1[pt];
+      pc[2] = Q2[pt];
     }
   };
   prefetch(k0 + R, k0);
-  constexpr int nhalo = 2 * R * (TX + TY);
   for (int k = k0; k < k1; ++k) {
-    if (pf_k >= 0) put_ring(k + R, pf, pf[5], pf[6], pf[7]);
+    if (pf_ok) put_ring(k + R, pf);
     const int slot = k % NS;
-    const double rho_c = pc[0], ir_c = 1.0 / pc[0];
+    const double rho_c = pc[0];
+    const double ir = 1.0 / rho_c;                            // ns_rho_rhou_p.f90:294
+    const double u1 = pc[1] * ir, u2 = pc[2] * ir;
     {
       T *c = plane + (ty + R) * PW + (tx + R);
+      const T *rp = ring + slot * NRF * RS + tid;
 #pragma unroll
-      for (int v = 0; v < 6; ++v) c[v * PS] = *ring_at(slot, v);
-      c[6 * PS] = pc[1] * ir_c;
-      c[7 * PS] = pc[2] * ir_c;
+      for (int f = 0; f < 6; ++f) c[f * PS] = rp[f * RS];
+      c[6 * PS] = u1;
+      c[7 * PS] = u2;
     }
     prefetch(k + R + 1, k + 1);
-    for (int h = tid; h < nhalo; h += TX * TY) {
-      int lx, ly;
-      if (h < 2 * R * TY) {
-        const int side = h / (R * TY), e = h % (R * TY);
-        ly = e / R;
-        lx = side == 0 ? -R + e % R : TX + e % R;
-      } else {
-        const int e2 = h - 2 * R * TY;
-        const int side = e2 / (R * TX), e = e2 % (R * TX);
-        lx = e % TX;
-        ly = side == 0 ? -R + e / TX : TY + e / TX;
-      }
-      const int hi = gidx(ox, i0 + lx), hj = gidx(oy, j0 + ly);
-      if (hi < 0 || hj < 0) continue;
-      const long long pt = hi + n1 * hj + n12 * k;
-      T *c = plane + (ly + R) * PW + (lx + R);
+    const long long kofs = (long long)n12 * k;
+    // epilogue inputs of this plane, issued before the barrier so their latency overlaps the stencils
+    const long long opt = (i0 + tx) + (long long)n1 * (j0 + ty) + kofs;
+    double e_src[5] = {0, 0, 0, 0, 0}, e_q0[5] = {0, 0, 0, 0, 0}, e_acc[5] = {0, 0, 0, 0, 0};
+    if (inside) {
+      if (a.src) {
 #pragma unroll
-      for (int v = 0; v < 5; ++v) c[v * PS] = a.qs[pt + v * N];
-      const double ir = 1.0 / a.q[pt];
-      c[5 * PS] = a.q[pt + 4 * N];
-      c[6 * PS] = a.q[pt + N] * ir;
-      c[7 * PS] = a.q[pt + 2 * N] * ir;
+        for (int v = 0; v < 5; ++v) e_src[v] = a.src[opt + v * N];
+      }
+      if (a.stage != 0) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) e_q0[v] = a.q0[opt + v * N];
+      }
+      if (a.stage >= 2) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) e_acc[v] = a.acc[opt + v * N];
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < HaloSet<R>::PER_THREAD; ++h) {
+      if (hs.goff[h] < 0) continue;
+      const long long pt = hs.goff[h] + kofs;
+      T *c = plane + hs.cell[h];
+      c[0 * PS] = S0[pt]; c[1 * PS] = S1[pt]; c[2 * PS] = S2[pt]; c[3 * PS] = S3[pt]; c[4 * PS] = S4[pt];
+      const double hir = 1.0 / Q0[pt];
+      c[5 * PS] = Q4[pt];
+      c[6 * PS] = Q1[pt] * hir;
+      c[7 * PS] = Q2[pt] * hir;
     }
     __syncthreads();
     if (inside) {
       const int i = i0 + tx, j = j0 + ty;
       const T *c = plane + (ty + R) * PW + (tx + R);
-      T zq[5][NS], zp[NS], zw[NS];
+      int so[NS];
 #pragma unroll
-      for (int m = -R; m <= R; ++m) {
-        const int sl = (slot + m + NS) % NS;
-#pragma unroll
-        for (int v = 0; v < 5; ++v) zq[v][m + R] = *ring_at(sl, v);
-        zp[m + R] = *ring_at(sl, 5);
-        zw[m + R] = *ring_at(sl, 6);
-      }
-      const double u1 = c[6 * PS], u2 = c[7 * PS], u3 = zw[R];
-      const double qs5 = zq[4][R];
+      for (int m = -R; m <= R; ++m) so[m + R] = ((slot + m + NS) % NS) * NRF * RS + tid;
+      const double qs5 = c[4 * PS];
       const double gm1 = a.gamma - 1.0;
-      const double gpr = a.gamma * zp[R] / (rho_c * gm1);       // :293
-      const double ir = 1.0 / rho_c;                            // :294
+      const double u3 = ring[so[R] + 6 * RS];
+      const double gpr = a.gamma * c[5 * PS] / (rho_c * gm1);   // :293
       double r1 = 0.0, r2 = 0.0, r3 = 0.0, r4 = 0.0, r5 = 0.0;  // :296
       {
         const double s = ox.scale;
-        const double A = dsm<T, R>(ox, c, 1, i) * s, B = dsm<T, R>(ox, c + PS, 1, i) * s,
-                     Cc = dsm<T, R>(ox, c + 2 * PS, 1, i) * s, D = dsm<T, R>(ox, c + 3 * PS, 1, i) * s,
-                     E = dsm<T, R>(ox, c + 4 * PS, 1, i) * s;
-        const double S = dsm2<T, R>(ox, c + 6 * PS, c + 4 * PS, 1, i) * s;
-        const double P = dsm<T, R>(ox, c + 5 * PS, 1, i) * s;
-        adj_dir(0, u1, u2, u3, gpr, ir, qs5, a.gamma, A, B, Cc, D, E, S, P, r1, r2, r3, r4, r5);
+        const double A = D1<T, R, PER>(ox, c, 1, i) * s, B = D1<T, R, PER>(ox, c + PS, 1, i) * s,
+                     Cc = D1<T, R, PER>(ox, c + 2 * PS, 1, i) * s, D = D1<T, R, PER>(ox, c + 3 * PS, 1, i) * s,
+                     E = D1<T, R, PER>(ox, c + 4 * PS, 1, i) * s;
+        const double Sx = D2<T, R, PER>(ox, c + 6 * PS, c + 4 * PS, 1, i) * s;
+        const double P = D1<T, R, PER>(ox, c + 5 * PS, 1, i) * s;
+        adj_dir(0, u1, u2, u3, gpr, ir, qs5, a.gamma, A, B, Cc, D, E, Sx, P, r1, r2, r3, r4, r5);
       }
       {
         const double s = oy.scale;
-        const double A = dsm<T, R>(oy, c, PW, j) * s, B = dsm<T, R>(oy, c + PS, PW, j) * s,
-                     Cc = dsm<T, R>(oy, c + 2 * PS, PW, j) * s, D = dsm<T, R>(oy, c + 3 * PS, PW, j) * s,
-                     E = dsm<T, R>(oy, c + 4 * PS, PW, j) * s;
-        const double S = dsm2<T, R>(oy, c + 7 * PS, c + 4 * PS, PW, j) * s;
-        const double P = dsm<T, R>(oy, c + 5 * PS, PW, j) * s;
-        adj_dir(1, u1, u2, u3, gpr, ir, qs5, a.gamma, A, B, Cc, D, E, S, P, r1, r2, r3, r4, r5);
+        const double A = D1<T, R, PER>(oy, c, PW, j) * s, B = D1<T, R, PER>(oy, c + PS, PW, j) * s,
+                     Cc = D1<T, R, PER>(oy, c + 2 * PS, PW, j) * s, D = D1<T, R, PER>(oy, c + 3 * PS, PW, j) * s,
+                     E = D1<T, R, PER>(oy, c + 4 * PS, PW, j) * s;
+        const double Sy = D2<T, R, PER>(oy, c + 7 * PS, c + 4 * PS, PW, j) * s;
+        const double P = D1<T, R, PER>(oy, c + 5 * PS, PW, j) * s;
+        adj_dir(1, u1, u2, u3, gpr, ir, qs5, a.gamma, A, B, Cc, D, E, Sy, P, r1, r2, r3, r4, r5);
       }
       {
         const double s = oz.scale;
-        const double A = dsz<T, R>(oz, zq[0], k) * s, B = dsz<T, R>(oz, zq[1], k) * s,
-                     Cc = dsz<T, R>(oz, zq[2], k) * s, D = dsz<T, R>(oz, zq[3], k) * s,
-                     E = dsz<T, R>(oz, zq[4], k) * s;
-        const double S = dsz2<T, R>(oz, zw, zq[4], k) * s;
-        const double P = dsz<T, R>(oz, zp, k) * s;
-        adj_dir(2, u1, u2, u3, gpr, ir, qs5, a.gamma, A, B, Cc, D, E, S, P, r1, r2, r3, r4, r5);
+        T zc[NS], zq5[NS];
+        double Z[5];
+#pragma unroll
+        for (int m = 0; m < NS; ++m) zq5[m] = ring[so[m] + 4 * RS];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+#pragma unroll
+          for (int m = 0; m < NS; ++m) zc[m] = ring[so[m] + f * RS];
+          Z[f] = Dz1<T, R, PER>(oz, zc, k) * s;
+        }
+        Z[4] = Dz1<T, R, PER>(oz, zq5, k) * s;
+#pragma unroll
+        for (int m = 0; m < NS; ++m) zc[m] = ring[so[m] + 6 * RS];
+        const double Sz = Dz2<T, R, PER>(oz, zc, zq5, k) * s;
+#pragma unroll
+        for (int m = 0; m < NS; ++m) zc[m] = ring[so[m] + 5 * RS];
+        const double P = Dz1<T, R, PER>(oz, zc, k) * s;
+        adj_dir(2, u1, u2, u3, gpr, ir, qs5, a.gamma, Z[0], Z[1], Z[2], Z[3], Z[4], Sz, P, r1, r2, r3, r4, r5);
       }
-      const long long pt = i + n1 * j + n12 * k;
       if (a.src) {                                              // :512
-        r1 = r1 + a.src[pt]; r2 = r2 + a.src[pt + N]; r3 = r3 + a.src[pt + 2 * N];
-        r4 = r4 + a.src[pt + 3 * N]; r5 = r5 + a.src[pt + 4 * N];
+        r1 = r1 + e_src[0]; r2 = r2 + e_src[1]; r3 = r3 + e_src[2]; r4 = r4 + e_src[3]; r5 = r5 + e_src[4];
       }
       const double kv[5] = {r1, r2, r3, r4, r5};
       if (a.stage == 0) {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) a.rhs[pt + v * N] = kv[v];
+        for (int v = 0; v < 5; ++v) a.rhs[opt + v * N] = kv[v];
       } else {
         const double dt = a.dt, dth = a.dt * 0.5;
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          const long long o = pt + v * N;
-          const double q0 = a.q0[o];
+          const long long o = opt + v * N;
           if (a.stage == 1) {
             a.acc[o] = kv[v];
-            a.qnext[o] = q0 + dth * kv[v];
+            a.qnext[o] = e_q0[v] + dth * kv[v];
           } else if (a.stage == 2) {
-            a.acc[o] = a.acc[o] + 2.0 * kv[v];
-            a.qnext[o] = q0 + dth * kv[v];
+            a.acc[o] = e_acc[v] + 2.0 * kv[v];
+            a.qnext[o] = e_q0[v] + dth * kv[v];
           } else if (a.stage == 3) {
-            a.acc[o] = a.acc[o] + 2.0 * kv[v];
-            a.qnext[o] = q0 + dt * kv[v];
+            a.acc[o] = e_acc[v] + 2.0 * kv[v];
+            a.qnext[o] = e_q0[v] + dt * kv[v];
           } else {
-            a.qnext[o] = q0 + dt / 6.0 * (a.acc[o] + kv[v]);
+            a.qnext[o] = e_q0[v] + dt / 6.0 * (e_acc[v] + kv[v]);
           }
         }
       }
@@ -252,11 +262,11 @@ size_t smem_adj() {
   return sizeof(double) * (8 * (TX + 2 * R) * (TY + 2 * R) + ring_slots(R) * 7 * TX * TY);
 }
 
-template <int R>
+template <int R, bool PER>
 void launch_adj(cruna_ctx *c, AdjArgs &a) {
   static bool configured = false;
   if (!configured) {
-    CRUNA_CUDA_CHECK(cudaFuncSetAttribute(k_adj_pass<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CRUNA_CUDA_CHECK(cudaFuncSetAttribute(k_adj_pass<R, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem_adj<R>()));
     configured = true;
   }
@@ -268,7 +278,7 @@ void launch_adj(cruna_ctx *c, AdjArgs &a) {
   nz = (n3 + kc - 1) / kc;
   a.kc = kc;
   ProfScope ps(c, "adj_pass");
-  k_adj_pass<R><<<dim3(bx, by, nz), dim3(TX, TY), smem_adj<R>(), c->stream>>>(a);
+  k_adj_pass<R, PER><<<dim3(bx, by, nz), dim3(TX, TY), smem_adj<R>(), c->stream>>>(a);
   CRUNA_LAUNCH_CHECK(c);
 }
 
@@ -299,8 +309,16 @@ void rhs_adjoint_fused(cruna_ctx *c, const double *qs_in, const double *q, const
   a.rhs = (stage == 0 || split) ? rhs : nullptr;
   int R = 0;
   for (int d = 0; d < 3; ++d) R = std::max(R, halo_of(c->dop[d]));
-  if (R <= 2) launch_adj<2>(c, a);
-  else launch_adj<4>(c, a);
+  const int Rl = R <= 2 ? 2 : 4;
+  bool per = true;
+  for (int d = 0; d < 3; ++d) per = per && c->dop[d].kind == OP_STENCIL && c->dop[d].periodic && c->dop[d].r == Rl;
+  if (Rl == 2) {
+    if (per) launch_adj<2, true>(c, a);
+    else launch_adj<2, false>(c, a);
+  } else {
+    if (per) launch_adj<4, true>(c, a);
+    else launch_adj<4, false>(c, a);
+  }
   if (stage == 0 || split) {
     if (c->has_rhs_bc) bc_rhss(c, rhs, qs, nullptr);                // :518 (without q)
     if (split) rk_stage(c, stage, dt, rhs, qs0, acc, qnext);

@@ -174,6 +174,87 @@ __device__ __forceinline__ int gidx(const DirOpF &op, int g) {
 }
 
 
+
+// ---- compile-time specialised evaluators -------------------------------------------------------
+// PER = true: every direction is periodic with half-width exactly R, so the stencil needs no
+// boundary logic and no predicates; PER = false falls back to the run-time operator (closures,
+// empty directions, smaller half-widths).
+template <typename T, int R>
+__device__ __forceinline__ T dper(const DirOpF &op, const T *p, int s) {
+  T t = T(op.c[1]) * (p[s] - p[-s]);
+#pragma unroll
+  for (int m = 2; m <= R; ++m) t = t + T(op.c[m]) * (p[m * s] - p[-m * s]);
+  return t;
+}
+template <typename T, int R>
+__device__ __forceinline__ T dper2(const DirOpF &op, const T *a, const T *b, int s) {
+  T t = T(op.c[1]) * (a[s] * b[s] - a[-s] * b[-s]);
+#pragma unroll
+  for (int m = 2; m <= R; ++m) t = t + T(op.c[m]) * (a[m * s] * b[m * s] - a[-m * s] * b[-m * s]);
+  return t;
+}
+template <typename T, int R, bool PER>
+__device__ __forceinline__ T D1(const DirOpF &op, const T *p, int s, int i) {
+  if constexpr (PER) return dper<T, R>(op, p, s);
+  else return dsm<T, R>(op, p, s, i);
+}
+template <typename T, int R, bool PER>
+__device__ __forceinline__ T D2(const DirOpF &op, const T *a, const T *b, int s, int i) {
+  if constexpr (PER) return dper2<T, R>(op, a, b, s);
+  else return dsm2<T, R>(op, a, b, s, i);
+}
+// z versions on register columns v[0..2R] centred at v[R]
+template <typename T, int R, bool PER>
+__device__ __forceinline__ T Dz1(const DirOpF &op, const T *v, int k) {
+  if constexpr (PER) return dper<T, R>(op, v + R, 1);
+  else return dsz<T, R>(op, v, k);
+}
+template <typename T, int R, bool PER>
+__device__ __forceinline__ T Dz2(const DirOpF &op, const T *a, const T *b, int k) {
+  if constexpr (PER) return dper2<T, R>(op, a + R, b + R, 1);
+  else return dsz2<T, R>(op, a, b, k);
+}
+
+// halo strip cell h (no corners) of a TX x TY tile with R-wide halos -> local (lx, ly)
+template <int R>
+__device__ __forceinline__ void halo_cell(int h, int &lx, int &ly) {
+  if (h < 2 * R * TY) {
+    const int side = h / (R * TY), e = h % (R * TY);
+    ly = e / R;
+    lx = side == 0 ? -R + e % R : TX + e % R;
+  } else {
+    const int e2 = h - 2 * R * TY;
+    const int side = e2 / (R * TX), e = e2 % (R * TX);
+    lx = e % TX;
+    ly = side == 0 ? -R + e / TX : TY + e / TX;
+  }
+}
+
+// per-thread halo cells: smem cell offset and in-plane global offset (-1: outside an open line)
+template <int R>
+struct HaloSet {
+  static constexpr int NH = 2 * R * (TX + TY);
+  static constexpr int PER_THREAD = (NH + TX * TY - 1) / (TX * TY);
+  int cell[PER_THREAD];
+  int goff[PER_THREAD];
+  __device__ __forceinline__ void init(const DirOpF &ox, const DirOpF &oy, int i0, int j0, int tid, int n1) {
+    constexpr int PW = TX + 2 * R;
+#pragma unroll
+    for (int c = 0; c < PER_THREAD; ++c) {
+      const int h = tid + c * TX * TY;
+      cell[c] = -1;
+      goff[c] = -1;
+      if (h < NH) {
+        int lx, ly;
+        halo_cell<R>(h, lx, ly);
+        const int hi = gidx(ox, i0 + lx), hj = gidx(oy, j0 + ly);
+        cell[c] = (ly + R) * PW + (lx + R);
+        if (hi >= 0 && hj >= 0) goff[c] = hi + n1 * hj;
+      }
+    }
+  }
+};
+
 DirOpF to_dir(const LineOp &op, double dx, bool heat_dx);
 int halo_of(const LineOp &op);
 

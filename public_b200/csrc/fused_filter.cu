@@ -3,21 +3,19 @@
 // counterpart: the interior stencil of filter_pen_core_o10_i_c_o.f90:182-199 at alpha = 0 with
 // periodic wrap, blended q <- q - s*(q - F q)).
 //
-// One z-marching pass applies the three directional filters in the reference's order to all five
-// variables: each plane is loaded once with an R = 5 halo (corners included), x-filtered on the
-// halo rows, y-filtered into a per-thread z column of 2R+1 planes, and z-filtered from that column.
-// The output goes to a second buffer (the filter reads neighbours), so the state is read and written
-// once per step instead of twice per direction.
+// Two passes apply the three directional filters in the reference's order to all five variables:
+// pass 1 filters each plane in x and then y on 32 x 32 tiles with 5-wide halos (corners included,
+// so the y filter sees x-filtered halo rows); pass 2 filters in z with a per-thread register queue
+// of 11 planes.  Each pass reads and writes the state once.
 #include "cruna_internal.cuh"
 #include "fused_common.cuh"
 
 namespace cruna {
 
-using namespace fz;
-
 namespace {
 
 constexpr int FR = 5;    // o10 filter half-width
+constexpr int FXT = 32, FYT = 32, FTHR = 256;
 
 struct FilterArgs {
   Grid g;
@@ -40,79 +38,70 @@ __device__ __forceinline__ double filt(const FilterArgs &a, const double *p, int
   return p[0] - a.blend * (p[0] - t);
 }
 
-__global__ void __launch_bounds__(TX *TY, 2) k_filter3(const __grid_constant__ FilterArgs a) {
-  constexpr int PW = TX + 2 * FR, PH = TY + 2 * FR, PS = PW * PH;
-  constexpr int XS = TX * PH;           // x-filtered rows (all y incl. halo) per variable
-  constexpr int NS = 2 * FR + 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double *raw = reinterpret_cast<double *>(smem_raw);   // [5][PH][PW]
-  double *xf = raw + 5 * PS;                            // [5][PH][TX]
-  double *ring = xf + 5 * XS;                           // [NS][5][TY*TX]
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-  const int k0 = blockIdx.z * a.kc;
-  const int k1 = min(k0 + a.kc, a.g.n3);
+// pass 1: x then y filter of one plane, one variable at a time
+__global__ void __launch_bounds__(FTHR) k_filter_xy(const __grid_constant__ FilterArgs a) {
+  constexpr int PW = FXT + 2 * FR, PH = FYT + 2 * FR;
+  __shared__ double raw[PH * PW];
+  __shared__ double xf[PH * FXT];
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * FXT, j0 = blockIdx.y * FYT, k = blockIdx.z;
   const long long N = a.g.N, n1 = a.g.n1, n12 = (long long)a.g.n1 * a.g.n2;
-  const bool inside = (i0 + tx) < a.g.n1 && (j0 + ty) < a.g.n2;
+  const long long kofs = n12 * k;
+  for (int v = 0; v < 5; ++v) {
+    const double *in = a.in + v * N;
+    double *out = a.out + v * N;
+    for (int c = tid; c < PW * PH; c += FTHR) {
+      const int lx = c % PW - FR, ly = c / PW - FR;
+      const int gi = a.on[0] ? wrapi(i0 + lx, a.n[0]) : min(max(i0 + lx, 0), a.n[0] - 1);
+      const int gj = a.on[1] ? wrapi(j0 + ly, a.n[1]) : min(max(j0 + ly, 0), a.n[1] - 1);
+      raw[c] = in[gi + n1 * gj + kofs];
+    }
+    __syncthreads();
+    for (int c = tid; c < FXT * PH; c += FTHR) {
+      const int lx = c % FXT, ly = c / FXT;
+      const double *p = raw + ly * PW + lx + FR;
+      xf[c] = a.on[0] ? filt(a, p, 1) : p[0];
+    }
+    __syncthreads();
+    for (int c = tid; c < FXT * FYT; c += FTHR) {
+      const int lx = c % FXT, ly = c / FXT;
+      const int gi = i0 + lx, gj = j0 + ly;
+      if (gi < a.g.n1 && gj < a.g.n2) {
+        const double *p = xf + (ly + FR) * FXT + lx;
+        out[gi + n1 * gj + kofs] = a.on[1] ? filt(a, p, FXT) : p[0];
+      }
+    }
+    __syncthreads();
+  }
+}
 
-  // filters plane kk of the input in x then y into ring slot kk (this thread's column)
-  auto xy_plane = [&](int kk) {
-    const int gk = a.on[2] ? wrapi(kk, a.n[2]) : kk;
-    const bool valid = gk >= 0 && gk < a.n[2];
-    __syncthreads();
-    if (valid) {
-      for (int cidx = tid; cidx < PW * PH; cidx += TX * TY) {
-        const int lx = cidx % PW - FR, ly = cidx / PW - FR;
-        const int gi = a.on[0] ? wrapi(i0 + lx, a.n[0]) : min(max(i0 + lx, 0), a.n[0] - 1);
-        const int gj = a.on[1] ? wrapi(j0 + ly, a.n[1]) : min(max(j0 + ly, 0), a.n[1] - 1);
-        const long long pt = gi + n1 * gj + n12 * gk;
+// pass 2: z filter with a per-thread register queue of 2*FR+1 planes (one variable at a time)
+__global__ void __launch_bounds__(FTHR) k_filter_z(const __grid_constant__ FilterArgs a) {
+  constexpr int NQ = 2 * FR + 1;
+  const int i = blockIdx.x * 32 + threadIdx.x % 32, j = blockIdx.y * 8 + threadIdx.x / 32;
+  if (i >= a.g.n1 || j >= a.g.n2) return;
+  const int k0 = blockIdx.z * a.kc, k1 = min(k0 + a.kc, a.g.n3);
+  const long long N = a.g.N, n12 = (long long)a.g.n1 * a.g.n2;
+  const long long col = i + (long long)a.g.n1 * j;
+  const int n3 = a.n[2];
+  for (int v = 0; v < 5; ++v) {
+    const double *in = a.in + v * N + col;
+    double *out = a.out + v * N + col;
+    double q[NQ];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) raw[v * PS + cidx] = a.in[pt + v * N];
-      }
-    }
-    __syncthreads();
-    if (valid) {
-      for (int cidx = tid; cidx < TX * PH; cidx += TX * TY) {
-        const int lx = cidx % TX, ly = cidx / TX;          // ly in [0, PH)
-        const double *p = raw + ly * PW + (lx + FR);
+    for (int m = 0; m < NQ - 1; ++m) q[m] = in[n12 * wrapi(k0 - FR + m, n3)];
+    for (int k = k0; k < k1; ++k) {
+      q[NQ - 1] = in[n12 * wrapi(k + FR, n3)];
+      out[n12 * k] = filt(a, q + FR, 1);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) xf[v * XS + cidx] = a.on[0] ? filt(a, p + v * PS, 1) : p[v * PS];
-      }
-    }
-    __syncthreads();
-    if (valid) {
-      const int sl = ((kk % NS) + NS) % NS;
-      const double *p = xf + (ty + FR) * TX + tx;
-#pragma unroll
-      for (int v = 0; v < 5; ++v)
-        ring[(sl * 5 + v) * (TX * TY) + tid] = a.on[1] ? filt(a, p + v * XS, TX) : p[v * XS];
-    }
-  };
-  for (int kk = k0 - FR; kk < k0 + FR; ++kk) xy_plane(kk);
-  for (int k = k0; k < k1; ++k) {
-    xy_plane(k + FR);
-    if (inside) {
-      const int slot = k % NS;
-      const long long pt = (i0 + tx) + n1 * (j0 + ty) + n12 * k;
-#pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        double col[NS];
-#pragma unroll
-        for (int m = -FR; m <= FR; ++m) col[m + FR] = ring[(((slot + m + NS) % NS) * 5 + v) * (TX * TY) + tid];
-        a.out[pt + v * N] = a.on[2] ? filt(a, col + FR, 1) : col[FR];
-      }
+      for (int m = 0; m < NQ - 1; ++m) q[m] = q[m + 1];
     }
   }
 }
 
-size_t smem_filter3() {
-  return sizeof(double) *
-         (5 * (TX + 2 * FR) * (TY + 2 * FR) + 5 * TX * (TY + 2 * FR) + (2 * FR + 1) * 5 * TX * TY);
-}
-
 }  // namespace
 
-// filters usable by the fused pass: the explicit periodic o10 filter or none, in every direction
+// filters usable by the fused passes: the explicit periodic o10 filter or none, in every direction
 bool filter_fused_supported(const cruna_ctx *c) {
   double ref[FR + 1] = {0};
   bool have = false;
@@ -122,7 +111,7 @@ bool filter_fused_supported(const cruna_ctx *c) {
     if (!(op.periodic && !op.solve && op.r == FR && op.blend > 0.0)) return false;
     if (have) {
       for (int m = 0; m <= FR; ++m)
-        if (op.c[m] != ref[m]) return false;
+        if (op.c[m] != ref[m] || op.blend != c->fop[0].blend) return false;
     } else {
       for (int m = 0; m <= FR; ++m) ref[m] = op.c[m];
       have = true;
@@ -131,7 +120,8 @@ bool filter_fused_supported(const cruna_ctx *c) {
   return true;
 }
 
-// out = filter_i3(filter_i2(filter_i1(in))) restricted to the directions with on[d] != 0
+// out = filter_i3(filter_i2(filter_i1(in))) restricted to the directions with on[d] != 0; in != out.
+// Uses the stage buffer st[0] as the intermediate between the two passes.
 void filter3_fused(cruna_ctx *c, const double *in, double *out, const int on_in[3]) {
   FilterArgs a;
   a.g = c->g;
@@ -150,24 +140,30 @@ void filter3_fused(cruna_ctx *c, const double *in, double *out, const int on_in[
       for (int m = 0; m <= FR; ++m) a.c[m] = c->fop[d].c[m];
       a.blend = c->fop[d].blend;
     }
-  a.in = in;
-  a.out = out;
-  static bool configured = false;
-  if (!configured) {
-    CRUNA_CUDA_CHECK(
-        cudaFuncSetAttribute(k_filter3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_filter3()));
-    configured = true;
+  double *tmp = c->st[0];
+  const double *src = in;
+  a.kc = 1;
+  if (a.on[0] || a.on[1]) {
+    a.in = src;
+    a.out = a.on[2] ? tmp : out;
+    const int bx = (c->g.n1 + FXT - 1) / FXT, by = (c->g.n2 + FYT - 1) / FYT;
+    ProfScope ps(c, "filter_xy");
+    k_filter_xy<<<dim3(bx, by, c->g.n3), FTHR, 0, c->stream>>>(a);
+    CRUNA_LAUNCH_CHECK(c);
+    src = tmp;
   }
-  const int bx = (c->g.n1 + TX - 1) / TX, by = (c->g.n2 + TY - 1) / TY;
-  const int n3 = c->g.n3;
-  int nz = std::max(1, std::min(n3, (4 * 148 + bx * by - 1) / (bx * by)));
-  int kc = (n3 + nz - 1) / nz;
-  kc = std::max(kc, std::min(n3, 4 * FR));
-  nz = (n3 + kc - 1) / kc;
-  a.kc = kc;
-  ProfScope ps(c, "filter3");
-  k_filter3<<<dim3(bx, by, nz), dim3(TX, TY), smem_filter3(), c->stream>>>(a);
-  CRUNA_LAUNCH_CHECK(c);
+  if (a.on[2]) {
+    a.in = src;
+    a.out = out;
+    const int zx = (c->g.n1 + 31) / 32, zy = (c->g.n2 + 7) / 8;
+    const int n3 = c->g.n3;
+    int nz = std::max(1, std::min(std::max(1, n3 / 16), (8 * 148 + zx * zy - 1) / (zx * zy)));
+    a.kc = (n3 + nz - 1) / nz;
+    nz = (n3 + a.kc - 1) / a.kc;
+    ProfScope ps(c, "filter_z");
+    k_filter_z<<<dim3(zx, zy, nz), FTHR, 0, c->stream>>>(a);
+    CRUNA_LAUNCH_CHECK(c);
+  }
 }
 
 }  // namespace cruna
