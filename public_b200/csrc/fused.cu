@@ -91,6 +91,19 @@ __global__ void __launch_bounds__(TX *TY, 2) k_pass_g(const __grid_constant__ Fu
     }
   };
   prefetch(k0 + R, k0);
+  // raw state of this thread's halo cells, loaded one plane ahead
+  constexpr int NHT = HaloSet<R>::PER_THREAD;
+  double hv[NHT][5];
+  auto halo_fetch = [&](int kk) {
+    const long long kofs = (long long)n12 * kk;
+#pragma unroll
+    for (int h = 0; h < NHT; ++h) {
+      if (hs.goff[h] < 0) continue;
+      const long long pt = hs.goff[h] + kofs;
+      hv[h][0] = Q0[pt]; hv[h][1] = Q1[pt]; hv[h][2] = Q2[pt]; hv[h][3] = Q3[pt]; hv[h][4] = Q4[pt];
+    }
+  };
+  halo_fetch(k0);
 
   for (int k = k0; k < k1; ++k) {
     if (pf_ok) put_ring(k + R, pf[0], pf[1], pf[2], pf[3], pf[4]);
@@ -103,19 +116,19 @@ __global__ void __launch_bounds__(TX *TY, 2) k_pass_g(const __grid_constant__ Fu
       c[5 * PS] = T(pruv[0]);
       c[6 * PS] = T(pruv[1]);
     }
-    prefetch(k + R + 1, k + 1);
     const long long kofs = (long long)n12 * k;
 #pragma unroll
-    for (int h = 0; h < HaloSet<R>::PER_THREAD; ++h) {
+    for (int h = 0; h < NHT; ++h) {
       if (hs.goff[h] < 0) continue;
-      const long long pt = hs.goff[h] + kofs;
-      const double r = Q0[pt], ru = Q1[pt], rv = Q2[pt], rw = Q3[pt], p = Q4[pt];
+      const double r = hv[h][0], ru = hv[h][1], rv = hv[h][2], rw = hv[h][3], p = hv[h][4];
       const double ir = 1.0 / r;
       T *c = plane + hs.cell[h];
       c[0 * PS] = T(ru * ir); c[1 * PS] = T(rv * ir); c[2 * PS] = T(rw * ir);
       c[3 * PS] = T(a.WoR * p * ir - a.T_ref);
       c[4 * PS] = T(p - a.p_ref); c[5 * PS] = T(ru); c[6 * PS] = T(rv);
     }
+    prefetch(k + R + 1, k + 1);
+    if (k + 1 < k1) halo_fetch(k + 1);
     __syncthreads();
     if (inside) {
       const int i = i0 + tx, j = j0 + ty;
@@ -266,6 +279,19 @@ __global__ void __launch_bounds__(TX *TY, 2) k_pass_d(const __grid_constant__ Fu
     }
   };
   prefetch(k0 + R, k0);
+  constexpr int NHT = HaloSet<R>::PER_THREAD;
+  T hv[NHT][7];
+  auto halo_fetch = [&](int kk) {
+    const long long kofs = (long long)n12 * kk;
+#pragma unroll
+    for (int h = 0; h < NHT; ++h) {
+      if (hs.goff[h] < 0) continue;
+      const long long pt = hs.goff[h] + kofs;
+#pragma unroll
+      for (int f = 0; f < 7; ++f) hv[h][f] = G[pt + pfld[f] * N];
+    }
+  };
+  halo_fetch(k0);
   for (int k = k0; k < k1; ++k) {
     if (pf_ok) {
       T *rp = ring + (((k + R) % NS + NS) % NS) * NRF * RS + tid;
@@ -278,7 +304,6 @@ __global__ void __launch_bounds__(TX *TY, 2) k_pass_d(const __grid_constant__ Fu
 #pragma unroll
       for (int f = 0; f < 7; ++f) c[f * PS] = pc[f];
     }
-    prefetch(k + R + 1, k + 1);
     const long long kofs = (long long)n12 * k;
     // epilogue inputs of this plane, issued before the barrier so their latency overlaps the stencils
     const long long opt = (i0 + tx) + (long long)n1 * (j0 + ty) + kofs;
@@ -302,13 +327,14 @@ __global__ void __launch_bounds__(TX *TY, 2) k_pass_d(const __grid_constant__ Fu
       }
     }
 #pragma unroll
-    for (int h = 0; h < HaloSet<R>::PER_THREAD; ++h) {
+    for (int h = 0; h < NHT; ++h) {
       if (hs.goff[h] < 0) continue;
-      const long long pt = hs.goff[h] + kofs;
       T *c = plane + hs.cell[h];
 #pragma unroll
-      for (int f = 0; f < 7; ++f) c[f * PS] = G[pt + pfld[f] * N];
+      for (int f = 0; f < 7; ++f) c[f * PS] = hv[h][f];
     }
+    prefetch(k + R + 1, k + 1);
+    if (k + 1 < k1) halo_fetch(k + 1);
     __syncthreads();
     if (inside) {
       const int i = i0 + tx, j = j0 + ty;

@@ -131,6 +131,19 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
     }
   };
   prefetch(k0 + R, k0);
+  constexpr int NHT = HaloSet<R>::PER_THREAD;
+  double hv[NHT][9];      // qs1..qs5, rho, rho*u, rho*v, p of the halo cells, one plane ahead
+  auto halo_fetch = [&](int kk) {
+    const long long kofs = (long long)n12 * kk;
+#pragma unroll
+    for (int h = 0; h < NHT; ++h) {
+      if (hs.goff[h] < 0) continue;
+      const long long pt = hs.goff[h] + kofs;
+      hv[h][0] = S0[pt]; hv[h][1] = S1[pt]; hv[h][2] = S2[pt]; hv[h][3] = S3[pt]; hv[h][4] = S4[pt];
+      hv[h][5] = Q0[pt]; hv[h][6] = Q1[pt]; hv[h][7] = Q2[pt]; hv[h][8] = Q4[pt];
+    }
+  };
+  halo_fetch(k0);
   for (int k = k0; k < k1; ++k) {
     if (pf_ok) put_ring(k + R, pf);
     const int slot = k % NS;
@@ -145,7 +158,6 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
       c[6 * PS] = u1;
       c[7 * PS] = u2;
     }
-    prefetch(k + R + 1, k + 1);
     const long long kofs = (long long)n12 * k;
     // epilogue inputs of this plane, issued before the barrier so their latency overlaps the stencils
     const long long opt = (i0 + tx) + (long long)n1 * (j0 + ty) + kofs;
@@ -165,16 +177,18 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
       }
     }
 #pragma unroll
-    for (int h = 0; h < HaloSet<R>::PER_THREAD; ++h) {
+    for (int h = 0; h < NHT; ++h) {
       if (hs.goff[h] < 0) continue;
-      const long long pt = hs.goff[h] + kofs;
       T *c = plane + hs.cell[h];
-      c[0 * PS] = S0[pt]; c[1 * PS] = S1[pt]; c[2 * PS] = S2[pt]; c[3 * PS] = S3[pt]; c[4 * PS] = S4[pt];
-      const double hir = 1.0 / Q0[pt];
-      c[5 * PS] = Q4[pt];
-      c[6 * PS] = Q1[pt] * hir;
-      c[7 * PS] = Q2[pt] * hir;
+      c[0 * PS] = hv[h][0]; c[1 * PS] = hv[h][1]; c[2 * PS] = hv[h][2]; c[3 * PS] = hv[h][3];
+      c[4 * PS] = hv[h][4];
+      const double hir = 1.0 / hv[h][5];
+      c[5 * PS] = hv[h][8];
+      c[6 * PS] = hv[h][6] * hir;
+      c[7 * PS] = hv[h][7] * hir;
     }
+    prefetch(k + R + 1, k + 1);
+    if (k + 1 < k1) halo_fetch(k + 1);
     __syncthreads();
     if (inside) {
       const int i = i0 + tx, j = j0 + ty;

@@ -38,23 +38,42 @@ __device__ __forceinline__ double filt(const FilterArgs &a, const double *p, int
   return p[0] - a.blend * (p[0] - t);
 }
 
-// pass 1: x then y filter of one plane, one variable at a time
+// pass 1: x then y filter of one plane, one variable at a time (tile offsets computed once)
 __global__ void __launch_bounds__(FTHR) k_filter_xy(const __grid_constant__ FilterArgs a) {
   constexpr int PW = FXT + 2 * FR, PH = FYT + 2 * FR;
+  constexpr int NL = (PW * PH + FTHR - 1) / FTHR;
   __shared__ double raw[PH * PW];
   __shared__ double xf[PH * FXT];
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * FXT, j0 = blockIdx.y * FYT, k = blockIdx.z;
   const long long N = a.g.N, n1 = a.g.n1, n12 = (long long)a.g.n1 * a.g.n2;
   const long long kofs = n12 * k;
-  for (int v = 0; v < 5; ++v) {
-    const double *in = a.in + v * N;
-    double *out = a.out + v * N;
-    for (int c = tid; c < PW * PH; c += FTHR) {
+  int goff[NL];
+#pragma unroll
+  for (int m = 0; m < NL; ++m) {
+    const int c = tid + m * FTHR;
+    goff[m] = -1;
+    if (c < PW * PH) {
       const int lx = c % PW - FR, ly = c / PW - FR;
       const int gi = a.on[0] ? wrapi(i0 + lx, a.n[0]) : min(max(i0 + lx, 0), a.n[0] - 1);
       const int gj = a.on[1] ? wrapi(j0 + ly, a.n[1]) : min(max(j0 + ly, 0), a.n[1] - 1);
-      raw[c] = in[gi + n1 * gj + kofs];
+      goff[m] = gi + (int)n1 * gj;
+    }
+  }
+  double nxt[NL];
+#pragma unroll
+  for (int m = 0; m < NL; ++m)
+    if (goff[m] >= 0) nxt[m] = a.in[goff[m] + kofs];
+  for (int v = 0; v < 5; ++v) {
+    double *out = a.out + v * N;
+#pragma unroll
+    for (int m = 0; m < NL; ++m)
+      if (goff[m] >= 0) raw[tid + m * FTHR] = nxt[m];
+    if (v + 1 < 5) {
+      const double *in1 = a.in + (v + 1) * N;
+#pragma unroll
+      for (int m = 0; m < NL; ++m)
+        if (goff[m] >= 0) nxt[m] = in1[goff[m] + kofs];
     }
     __syncthreads();
     for (int c = tid; c < FXT * PH; c += FTHR) {
@@ -75,7 +94,8 @@ __global__ void __launch_bounds__(FTHR) k_filter_xy(const __grid_constant__ Filt
   }
 }
 
-// pass 2: z filter with a per-thread register queue of 2*FR+1 planes (one variable at a time)
+// pass 2: z filter with per-thread register queues of 2*FR+1 planes for the five variables, the next
+// plane loaded one step ahead
 __global__ void __launch_bounds__(FTHR) k_filter_z(const __grid_constant__ FilterArgs a) {
   constexpr int NQ = 2 * FR + 1;
   const int i = blockIdx.x * 32 + threadIdx.x % 32, j = blockIdx.y * 8 + threadIdx.x / 32;
@@ -84,18 +104,34 @@ __global__ void __launch_bounds__(FTHR) k_filter_z(const __grid_constant__ Filte
   const long long N = a.g.N, n12 = (long long)a.g.n1 * a.g.n2;
   const long long col = i + (long long)a.g.n1 * j;
   const int n3 = a.n[2];
-  for (int v = 0; v < 5; ++v) {
-    const double *in = a.in + v * N + col;
-    double *out = a.out + v * N + col;
-    double q[NQ];
+  const double *in = a.in + col;
+  double *out = a.out + col;
+  double q[5][NQ], nx[5];
 #pragma unroll
-    for (int m = 0; m < NQ - 1; ++m) q[m] = in[n12 * wrapi(k0 - FR + m, n3)];
-    for (int k = k0; k < k1; ++k) {
-      q[NQ - 1] = in[n12 * wrapi(k + FR, n3)];
-      out[n12 * k] = filt(a, q + FR, 1);
+  for (int m = 0; m < NQ - 1; ++m) {
+    const long long o = n12 * wrapi(k0 - FR + m, n3);
 #pragma unroll
-      for (int m = 0; m < NQ - 1; ++m) q[m] = q[m + 1];
+    for (int v = 0; v < 5; ++v) q[v][m] = in[v * N + o];
+  }
+  {
+    const long long o = n12 * wrapi(k0 + FR, n3);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) nx[v] = in[v * N + o];
+  }
+  for (int k = k0; k < k1; ++k) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) q[v][NQ - 1] = nx[v];
+    if (k + 1 < k1) {
+      const long long o = n12 * wrapi(k + 1 + FR, n3);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) nx[v] = in[v * N + o];
     }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) out[v * N + n12 * k] = filt(a, q[v] + FR, 1);
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+#pragma unroll
+      for (int m = 0; m < NQ - 1; ++m) q[v][m] = q[v][m + 1];
   }
 }
 
