@@ -207,6 +207,22 @@ int cruna_set_force_generic(cruna_ctx *ctx, int force_generic);
 /* Number of kernels this library enqueued since the context was created (for launch accounting). */
 int64_t cruna_kernel_launches(const cruna_ctx *ctx);
 
+/* Allocation-free direct RHS.  No counterpart in the reference: it exists for callers that cannot
+   allocate device memory where they evaluate the RHS -- a host whose device memory belongs to
+   another allocator (a framework's caching pool) or a time loop that must keep a fixed footprint
+   decided at start-up -- and therefore cannot create a context (cruna_init allocates).
+   It evaluates right_hand_side_direct_3d for the explicit derivative cores (FP64, no boundary table,
+   no forcing) from cfg alone: q and rhs are device pointers (n1*n2*n3*5 doubles each) on the
+   current device and the work is enqueued on `stream` (a cudaStream_t, NULL = default stream).
+   Its intermediate (15 doubles per point) is a static device array of 131072 points (15.7 MB) that
+   every GPU loading the library keeps until exit; larger grids are rejected with CRUNA_ERR_ARG.
+   The first call on a device resolves that array's address and sets kernel attributes: make it
+   before any stream capture.  All calls share the array, so calls that overlap on the GPU race;
+   serialise them (one stream, or events).  Each call overwrites every intermediate value it reads.
+   On failure a message is written to errbuf (errlen bytes, may be NULL). */
+int cruna_rhs_direct_noalloc(const cruna_config *cfg, const double *q, double *rhs, void *stream, char *errbuf,
+                             int errlen);
+
 /* Kernel timing: while enabled, each kernel family (fused passes, filters, stage updates, generic
    line operators) is bracketed by CUDA events on the context's stream.  cruna_profile_report drains
    them and writes lines "name launches total_ms" into buf; it returns the length of the full report. */

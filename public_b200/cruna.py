@@ -108,6 +108,7 @@ _SIGNATURES = {
     "cruna_kernel_launches": (C.c_int64, [_P]),
     "cruna_profile_enable": (_I, [_P, _I]),
     "cruna_profile_report": (_I, [_P, C.c_char_p, _I]),
+    "cruna_rhs_direct_noalloc": (_I, [C.POINTER(_Config), _P, _P, _P, C.c_char_p, _I]),
     "cruna_lapack_dgttrf": (_I, [_I, _P, _P, _P, _P, _P]),
     "cruna_lapack_dgttrs": (None, [_I, _P, _P, _P, _P, _P, _P]),
 }

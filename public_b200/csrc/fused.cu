@@ -566,3 +566,166 @@ void rhs_direct_fused(cruna_ctx *c, const double *q_in, double *rhs, int stage, 
 }
 
 }  // namespace cruna
+
+// ------------------------------------------------------------------------------------------------
+// Allocation-free variant of the fused direct RHS.
+//
+// Some callers cannot allocate device memory at the point where they need an RHS evaluation: a
+// host code whose device memory is owned by another allocator (a framework's caching pool, a
+// Fortran code that sizes every array once at start-up and forbids allocation in its time loop), or
+// an embedded solver that must run with a fixed, pre-planned footprint.  cruna_init allocates the
+// context's buffers and therefore does not serve them.  cruna_rhs_direct_noalloc evaluates the same
+// two fused passes with no context: the 15-field intermediate of pass G lives in the file-scope
+// device array below (kNoAllocMaxPoints points, 15.7 MB, held by every GPU that loads the library
+// until the process exits), and the caller passes the input state and the output RHS.
+// ------------------------------------------------------------------------------------------------
+namespace cruna {
+namespace {
+
+constexpr long long kNoAllocMaxPoints = 131072;          // e.g. 64 x 64 x 32 grid points
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_noalloc_scratch[NG * kNoAllocMaxPoints];
+double *g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};   // device address of the array, per device
+
+void noalloc_msg(char *buf, int len, const char *msg) {
+  if (!buf || len <= 0) return;
+  int i = 0;
+  for (; msg[i] && i < len - 1; ++i) buf[i] = msg[i];
+  buf[i] = 0;
+}
+
+template <int R, bool PER>
+cudaError_t noalloc_attrs() {
+  cudaError_t e = cudaFuncSetAttribute(k_pass_g<double, R, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_g<double, R>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_pass_d<double, R, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_d<double, R>());
+}
+
+template <int R, bool PER>
+void noalloc_launch(const FusedArgs &a, dim3 grid, cudaStream_t s) {
+  k_pass_g<double, R, PER><<<grid, dim3(TX, TY), smem_g<double, R>(), s>>>(a);
+  k_pass_d<double, R, PER><<<grid, dim3(TX, TY), smem_d<double, R>(), s>>>(a);
+}
+
+}  // namespace
+}  // namespace cruna
+
+extern "C" int cruna_rhs_direct_noalloc(const cruna_config *cfg, const double *q, double *rhs, void *stream,
+                                        char *errbuf, int errlen) {
+  using namespace cruna;
+  using namespace cruna::fz;
+  if (!cfg || !q || !rhs) {
+    noalloc_msg(errbuf, errlen, "null argument");
+    return CRUNA_ERR_ARG;
+  }
+  if (cfg->abi_version != CRUNA_ABI_VERSION) {
+    noalloc_msg(errbuf, errlen, "cruna_config.abi_version mismatch");
+    return CRUNA_ERR_ARG;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (cfg->n[d] < 1) {
+      noalloc_msg(errbuf, errlen, "geom.n must be >= 1");
+      return CRUNA_ERR_ARG;
+    }
+  const long long npts = (long long)cfg->n[0] * cfg->n[1] * cfg->n[2];
+  if (npts > kNoAllocMaxPoints) {
+    noalloc_msg(errbuf, errlen,
+                "grid too large for cruna_rhs_direct_noalloc: at most 131072 points (its static scratch)");
+    return CRUNA_ERR_ARG;
+  }
+  if (cfg->precision != CRUNA_FP64) {
+    noalloc_msg(errbuf, errlen, "cruna_rhs_direct_noalloc computes in FP64 only");
+    return CRUNA_ERR_UNSUPPORTED;
+  }
+  if (!(cfg->gamma > 1.0) || !(cfg->R > 0.0) || !(cfg->W > 0.0) || !(cfg->T0 > 0.0) || !(cfg->Pr > 0.0)) {
+    noalloc_msg(errbuf, errlen, "material.gamma must be > 1 and R, W, T0, Pr positive");
+    return CRUNA_ERR_ARG;
+  }
+  // explicit derivative cores only (the compact cores need factor arrays); built on the stack
+  LineOp ops[3];
+  for (int d = 0; d < 3; ++d) {
+    HostFactors hf;        // stays empty for explicit cores
+    std::string err;       // short messages only; not filled on success
+    if (!build_diff_op(cfg->diff[d], cfg->n[d], ops[d], hf, err)) {
+      noalloc_msg(errbuf, errlen, "unsupported derivative scheme or grid size for this direction");
+      return CRUNA_ERR_ARG;
+    }
+    if (ops[d].kind == OP_STENCIL && (ops[d].solve || ops[d].r > 4 || ops[d].nb > 2 || ops[d].bw > 5)) {
+      noalloc_msg(errbuf, errlen, "cruna_rhs_direct_noalloc supports the explicit derivative cores only");
+      return CRUNA_ERR_UNSUPPORTED;
+    }
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    cudaGetLastError();
+    noalloc_msg(errbuf, errlen, "no usable current CUDA device");
+    return CRUNA_ERR_NODEVICE;
+  }
+  // first call on this device: resolve the array's device address and set the kernels' shared-memory
+  // limits (host code must not pass the array's name to a kernel: it is only a host-side stand-in)
+  if (!g_noalloc_ptr[dev]) {
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e == cudaSuccess) e = noalloc_attrs<2, false>();
+    if (e == cudaSuccess) e = noalloc_attrs<2, true>();
+    if (e == cudaSuccess) e = noalloc_attrs<4, false>();
+    if (e == cudaSuccess) e = noalloc_attrs<4, true>();
+    if (e != cudaSuccess || !ptr) {
+      cudaGetLastError();
+      noalloc_msg(errbuf, errlen, "cudaGetSymbolAddress / cudaFuncSetAttribute failed during set-up");
+      return CRUNA_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = static_cast<double *>(ptr);
+  }
+  Grid g{cfg->n[0], cfg->n[1], cfg->n[2], npts};
+  FusedArgs a;
+  a.g = g;
+  for (int d = 0; d < 3; ++d) {
+    const double L = cfg->x1[d] - cfg->x0[d];                    // grid_transform.f90:40-56
+    const int m = diff_is_periodic(cfg->diff[d]) ? cfg->n[d] : cfg->n[d] - 1;
+    a.op[d] = to_dir(ops[d], m > 0 ? L / m : INFINITY, cfg->heat_flux_dx != 0);
+  }
+  a.WoR = cfg->W / cfg->R;
+  a.mu0 = cfg->mu0;
+  a.T0 = cfg->T0;
+  a.gamma = cfg->gamma;
+  a.cp_over_pr = cfg->gamma * (cfg->R / cfg->W) / (cfg->gamma - 1.0) / cfg->Pr;
+  a.p_ref = 0.0;
+  a.T_ref = 0.0;
+  a.q = q;
+  a.gbuf = g_noalloc_ptr[dev];      // every value of the 15 fields is written by pass G before use
+  a.rhs = rhs;
+  a.force = nullptr;
+  a.stage = 0;
+  a.dt = 0.0;
+  a.q0 = nullptr;
+  a.acc = nullptr;
+  a.qnext = nullptr;
+  int R = 0;
+  for (int d = 0; d < 3; ++d) R = std::max(R, halo_of(ops[d]));
+  const int Rl = R <= 2 ? 2 : 4;
+  bool per = true;
+  for (int d = 0; d < 3; ++d) per = per && ops[d].kind == OP_STENCIL && ops[d].periodic && ops[d].r == Rl;
+  const int bx = (g.n1 + TX - 1) / TX, by = (g.n2 + TY - 1) / TY;
+  int nz = std::max(1, std::min(g.n3, (4 * 148 + bx * by - 1) / (bx * by)));
+  int kc = (g.n3 + nz - 1) / nz;
+  kc = std::max(kc, std::min(g.n3, 4 * Rl));
+  nz = (g.n3 + kc - 1) / kc;
+  a.kc = kc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (Rl == 2) {
+    if (per) noalloc_launch<2, true>(a, dim3(bx, by, nz), s);
+    else noalloc_launch<2, false>(a, dim3(bx, by, nz), s);
+  } else {
+    if (per) noalloc_launch<4, true>(a, dim3(bx, by, nz), s);
+    else noalloc_launch<4, false>(a, dim3(bx, by, nz), s);
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    noalloc_msg(errbuf, errlen, cudaGetErrorString(e));
+    return CRUNA_ERR_CUDA;
+  }
+  return CRUNA_OK;
+}
