@@ -130,3 +130,22 @@ def test_sponge_shape_matches_reference_formula():
     assert abs(sh[0, 15, 0] - 3.0) < 1e-14           # at the x-boundary phi = 0 -> shape = amp
     assert abs(sh[10, 15, 0]) < 1e-14                  # interior: no sponge
     assert np.all(sh >= 0) and np.all(sh <= 3.0 + 1e-14)
+
+
+def test_cpu_twin_matches_oracle():
+    """The C + OpenMP restatement used as the timed CPU baseline reproduces the numpy oracle."""
+    from oracle import cpu_twin
+    s, q0 = cases.taylor_green(n=12, seed=2)
+    s["mu0"] = 0.02
+    s["ai_freq"] = (1, 1, 1)
+    fields = {f.name for f in O.dataclasses.fields(O.Config)}
+    S = O.Solver(O.Config(**{k: v for k, v in s.items() if k in fields}))
+    qs0 = cases.smooth_random_state((12, 12, 12), seed=3, p0=0.0, rho0=0.0, amp=1.0)
+    q, qs = q0.copy(order="F"), qs0.copy(order="F")
+    for it in range(2):
+        q = S.calc_direct(q, 1, nt0=it)
+        qs, _ = S.calc_adjoint(qs, [q, q])
+    qc, qsc = q0.copy(order="F"), qs0.copy(order="F")
+    cpu_twin.run(s, qc, qsc, 2, 2)
+    assert max(O.rel_l2(qc[..., v], q[..., v]) for v in range(5)) < 1e-12
+    assert max(O.rel_l2(qsc[..., v], qs[..., v]) for v in range(5)) < 1e-12
