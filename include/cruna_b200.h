@@ -195,6 +195,34 @@ int cruna_run_adjoint(cruna_ctx *ctx, double *qs_io, const double *Q_traj, const
 int cruna_run_adjoint_dev(cruna_ctx *ctx, double *qs_io, const double *Q_traj, const double *g_traj,
                           int nt_end, int nsteps);
 
+/*
+ * Objectives and gradients of CRUNA's optimisation loop (src/main/cruna.f90:78-179): calc_direct,
+ * calc_objective, calc_adjoint with calc_objective_g as the adjoint source, calc_grad.  The reference
+ * leaves objective and gradient to each case (src/opt/objective.f90:19-45, src/opt/force.f90:41-45);
+ * these are the library's built-in ones:
+ *   CRUNA_OBJ_PLANE_P2       J = sum_{nt=1..T} dt * sum_{plane x_normal = index} dA (p - p_inf)^2,
+ *                            adjoint source g = (0,0,0,0, 2 dA (p - p_inf)) on the plane
+ *   CRUNA_OBJ_KINETIC_ENERGY J = sum dV |rho u|^2 / (2 rho) at the final time, qs(T) = dJ/dq
+ */
+enum cruna_objective_kind { CRUNA_OBJ_PLANE_P2 = 1, CRUNA_OBJ_KINETIC_ENERGY = 2 };
+typedef struct cruna_objective {
+  int32_t kind;       /* enum cruna_objective_kind */
+  int32_t normal;     /* plane normal direction 1..3 (CRUNA_OBJ_PLANE_P2) */
+  int32_t index;      /* 1-based plane index */
+  int32_t reserved;
+  double p_inf;       /* reference pressure */
+} cruna_objective;
+
+/* J, dJ/df for the time-constant forcing set by cruna_set_forcing (the time integral of the adjoint
+   state, trapezoid rule) and dJ/dq0 = qs(0), from nsteps direct steps and the matching adjoint steps
+   of the run loops above.  The direct trajectory is recomputed from nsnap snapshots held in HBM
+   (binomial schedule, minimal recomputation; nsnap > nsteps keeps every state); *direct_steps
+   receives the number of direct steps executed.  grad_f / grad_q0 may be NULL. */
+int cruna_gradient(cruna_ctx *ctx, const double *q0, int nsteps, int nsnap, const cruna_objective *obj, double *J,
+                   double *grad_f, double *grad_q0, int64_t *direct_steps);
+int cruna_gradient_dev(cruna_ctx *ctx, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
+                       double *J, double *grad_f, double *grad_q0, int64_t *direct_steps);
+
 /* State check used by the run loops: returns CRUNA_ERR_STATE if any rho <= 0, p <= 0 or a
    non-finite value is found in q (device pointer). */
 int cruna_check_state_dev(cruna_ctx *ctx, const double *q);

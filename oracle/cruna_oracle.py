@@ -972,3 +972,149 @@ def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     """Relative L2 difference ||a-b|| / ||b||."""
     nb = float(np.linalg.norm(b.ravel()))
     return float(np.linalg.norm((a - b).ravel())) / (nb if nb > 0 else 1.0)
+
+
+# ------------------------------------------------------------------------------------------------
+# objectives and the gradient of CRUNA's optimisation loop (src/main/cruna.f90:78-179):
+# calc_direct -> calc_objective -> calc_adjoint (with calc_objective_g as the adjoint source) ->
+# calc_grad.  The reference leaves the objective and the gradient assembly to each case
+# (src/opt/objective.f90:19-45, force.f90:41-45); these are the library's built-in choices.
+# ------------------------------------------------------------------------------------------------
+def plane_weight(cfg: Config, normal: int) -> float:
+    """Area element of a grid plane with the given normal direction (0, 1, 2): product of the other
+    two grid spacings (a collapsed direction contributes 1)."""
+    dx = cfg.dx()
+    w = 1.0
+    for d in range(3):
+        if d != normal and cfg.n[d] > 1:
+            w *= dx[d]
+    return w
+
+
+def objective_plane_p2(cfg: Config, q: np.ndarray, normal: int, index: int, p_inf: float):
+    """j(q) = sum over the plane x_normal = index (0-based) of w (p - p_inf)^2 and its gradient
+    g = dj/dq (only the pressure component of the plane points is non-zero)."""
+    w = plane_weight(cfg, normal)
+    sl = [slice(None)] * 3
+    sl[normal] = index
+    p = q[..., 4][tuple(sl)]
+    dp = p - p_inf
+    j = float(np.sum(w * dp * dp))
+    g = np.zeros_like(q)
+    gp = g[..., 4]
+    gp[tuple(sl)] = 2.0 * w * dp
+    return j, g
+
+
+def objective_kinetic_energy(cfg: Config, q: np.ndarray):
+    """E(q) = sum dV * 0.5 |rho u|^2 / rho and dE/dq = dV * (-0.5|u|^2, u, v, w, 0)."""
+    dx = cfg.dx()
+    dV = 1.0
+    for d in range(3):
+        if cfg.n[d] > 1:
+            dV *= dx[d]
+    rho = q[..., 0]
+    m2 = q[..., 1] ** 2 + q[..., 2] ** 2 + q[..., 3] ** 2
+    E = float(np.sum(dV * 0.5 * m2 / rho))
+    g = np.zeros_like(q)
+    u = q[..., 1:4] / rho[..., None]
+    g[..., 0] = dV * (-0.5 * np.sum(u * u, axis=-1))
+    g[..., 1:4] = dV * u
+    return E, g
+
+
+def gradient_store_all(S: "Solver", q0: np.ndarray, steps: int, objective: dict):
+    """J, dJ/df (time-constant forcing) and dJ/dq0 with the whole trajectory stored.
+
+    objective = {"kind": "plane_p2", "normal": d, "index": i, "p_inf": p} gives
+    J = sum_{nt=1..steps} dt * j(Q(nt)) with the adjoint source g(Q(nt)) at adjoint step nt (the
+    order of computation_adjoint.f90:66-81); {"kind": "kinetic_energy"} gives J = E(Q(steps)) with
+    qs(T) = dE/dq.  dJ/df = integral of qs dt (trapezoid over the adjoint trajectory), dJ/dq0 = qs(0).
+    """
+    cfg = S.cfg
+    qT, Q = S.calc_direct(q0, steps, store=True)
+    J = 0.0
+    qs = np.zeros_like(q0)
+    gfn = None
+    if objective["kind"] == "plane_p2":
+        def gfn(qq, nt):
+            return objective_plane_p2(cfg, qq, objective["normal"], objective["index"], objective["p_inf"])[1]
+        for nt in range(1, steps + 1):
+            J += cfg.dt * objective_plane_p2(cfg, Q[nt], objective["normal"], objective["index"],
+                                             objective["p_inf"])[0]
+    else:
+        J, qs = objective_kinetic_energy(cfg, Q[steps])
+    qs_end, traj = S.calc_adjoint(qs, Q, g_fn=gfn)
+    gf = 0.5 * cfg.dt * traj[steps]
+    for nt in range(steps - 1, 0, -1):
+        gf = gf + cfg.dt * traj[nt]
+    gf = gf + 0.5 * cfg.dt * traj[0]
+    return J, np.asfortranarray(gf), qs_end
+
+
+def max_states(s: int, t: int) -> int:
+    """Most states rev() can reverse with s free snapshots and t sweeps: C(s+1+t, t) - 1."""
+    return math.comb(s + 1 + t, t) - 1
+
+
+def checkpoint_table(n: int, S: int):
+    """Minimal number of direct steps to reverse m <= n states with s <= S free snapshots, and the
+    first-checkpoint distance achieving it, searched within the binomial bounds."""
+    W = S + 1
+    cost = [[0] * W for _ in range(n + 1)]
+    kbest = [[1] * W for _ in range(n + 1)]
+    for s in range(W):
+        for m in range(1, n + 1):
+            if s == 0:
+                cost[m][s] = m * (m + 1) // 2
+                continue
+            t = 0
+            while max_states(s, t) < m:
+                t += 1
+            lo = max(1, m - max_states(s - 1, t))
+            hi = min(m, max_states(s, t - 1) + 1)
+            best, bk = None, lo
+            for k in range(lo, hi + 1):
+                v = k + cost[m - k][s - 1] + cost[k - 1][s]
+                if best is None or v < best:
+                    best, bk = v, k
+            cost[m][s], kbest[m][s] = best, bk
+    return cost, kbest
+
+
+def treeverse_schedule(steps: int, slots: int):
+    """Binomial checkpoint schedule to reverse `steps` time steps with `slots` snapshots (the state
+    Q(0) occupies one of them).  The adjoint step nt consumes Q(nt), nt = steps .. 1.  rev(a, b, s)
+    produces Q(b), ..., Q(a+1) from the stored Q(a) with s free slots: it advances to a checkpoint
+    a + k, reverses the right part with s - 1 slots, runs the adjoint step at the checkpoint from its
+    slot, then reverses the left part with s slots; k minimises the advanced steps.
+    Returns (actions, direct steps advanced)."""
+    if slots < 1:
+        raise ValueError("need at least one snapshot slot (for the initial state)")
+    S = min(slots - 1, steps)
+    _, kbest = checkpoint_table(steps, S)
+    acts = []
+
+    def rec(a, b, s):
+        n = b - a
+        if n <= 0:
+            return
+        if s == 0:
+            for nt in range(b, a, -1):
+                acts.append(("restore", a))
+                acts.append(("advance", a, nt))
+                acts.append(("adjoint", nt))
+            return
+        m = a + kbest[n][s]
+        acts.append(("restore", a))
+        acts.append(("advance", a, m))
+        acts.append(("store", m))
+        rec(m, b, s - 1)
+        acts.append(("restore", m))
+        acts.append(("adjoint", m))
+        acts.append(("free", m))
+        rec(a, m - 1, s)
+
+    rec(0, steps, S)
+    advanced = sum(r[1] - r[0] for (k, *r) in acts if k == "advance")
+    return acts, advanced

@@ -62,6 +62,12 @@ class _Config(C.Structure):
     ]
 
 
+class Objective(C.Structure):
+    """struct cruna_objective: kind 1 = plane (p - p_inf)^2 integral, kind 2 = final kinetic energy."""
+    _fields_ = [("kind", C.c_int32), ("normal", C.c_int32), ("index", C.c_int32), ("reserved", C.c_int32),
+                ("p_inf", C.c_double)]
+
+
 _P = C.c_void_p
 _D = C.c_double
 _I = C.c_int
@@ -109,6 +115,10 @@ _SIGNATURES = {
     "cruna_profile_enable": (_I, [_P, _I]),
     "cruna_profile_report": (_I, [_P, C.c_char_p, _I]),
     "cruna_rhs_direct_noalloc": (_I, [C.POINTER(_Config), _P, _P, _P, C.c_char_p, _I]),
+    "cruna_gradient": (_I, [_P, _P, _I, _I, C.POINTER(Objective), C.POINTER(C.c_double), _P, _P,
+                            C.POINTER(C.c_int64)]),
+    "cruna_gradient_dev": (_I, [_P, _P, _I, _I, C.POINTER(Objective), C.POINTER(C.c_double), _P, _P,
+                                C.POINTER(C.c_int64)]),
     "cruna_lapack_dgttrf": (_I, [_I, _P, _P, _P, _P, _P]),
     "cruna_lapack_dgttrs": (None, [_I, _P, _P, _P, _P, _P, _P]),
 }
@@ -393,6 +403,39 @@ class Cruna:
                                                _ptr(None if Gt is None else np.ascontiguousarray(Gt)),
                                                steps, steps))
         return a
+
+    @staticmethod
+    def objective(kind: str, normal: int = 2, index: int = 1, p_inf: float = 0.0) -> Objective:
+        """kind 'plane_p2' (normal, 1-based index, p_inf) or 'kinetic_energy'."""
+        o = Objective()
+        o.kind = {"plane_p2": 1, "kinetic_energy": 2}[kind]
+        o.normal, o.index, o.p_inf = int(normal), int(index), float(p_inf)
+        return o
+
+    def gradient(self, q0, nsteps: int, nsnap: int, objective: Objective):
+        """J, dJ/df, dJ/dq0 and the number of direct steps executed (binomial checkpointing)."""
+        a = self._state(q0)
+        gf = np.empty_like(a, order="F")
+        gq = np.empty_like(a, order="F")
+        J = C.c_double()
+        steps = C.c_int64()
+        self._check(self.lib.cruna_gradient(self.h, _ptr(a), int(nsteps), int(nsnap), C.byref(objective),
+                                            C.byref(J), _ptr(gf), _ptr(gq), C.byref(steps)))
+        return J.value, gf, gq, steps.value
+
+    def gradient_dev(self, q0_ptr: int, nsteps: int, nsnap: int, objective: Objective,
+                     grad_f_ptr: Optional[int], grad_q0_ptr: Optional[int]):
+        J = C.c_double()
+        steps = C.c_int64()
+        self._check(self.lib.cruna_gradient_dev(self.h, C.c_void_p(q0_ptr), int(nsteps), int(nsnap),
+                                                C.byref(objective), C.byref(J),
+                                                None if grad_f_ptr is None else C.c_void_p(grad_f_ptr),
+                                                None if grad_q0_ptr is None else C.c_void_p(grad_q0_ptr),
+                                                C.byref(steps)))
+        return J.value, steps.value
+
+    def set_forcing_dev(self, f_ptr: Optional[int]):
+        self._check(self.lib.cruna_set_forcing_dev(self.h, None if f_ptr is None else C.c_void_p(f_ptr)))
 
     # device-pointer variants (pointers from torch tensors or any CUDA allocation on the context's device)
     def rhs_direct_dev(self, q_ptr: int, rhs_ptr: int, t: float = 0.0):

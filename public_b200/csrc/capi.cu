@@ -736,21 +736,54 @@ int cruna_check_state_dev(cruna_ctx *c, const double *q) {
   });
 }
 
+}  // extern "C"
+
+namespace cruna {
+
+// one step of the loop body of calc_direct (computation_direct.f90:76-95): time_stepper_direct,
+// set_boundary_condition_q(outside_rhs) and the filters whose frequency divides nt; q in place
+void direct_loop_step(cruna_ctx *c, double *q, int nt) {
+  const int on[3] = {due(c->cfg.di_freq[0], nt), due(c->cfg.di_freq[1], nt), due(c->cfg.di_freq[2], nt)};
+  if (c->filter_fused_ok && !c->force_generic && (on[0] || on[1] || on[2])) {
+    step_direct(c, q, c->st[5]);
+    if (c->has_q_bc) bc_q(c, c->st[5], 1);
+    filter3_fused(c, c->st[5], q, on);
+  } else {
+    step_direct(c, q, q);
+    if (c->has_q_bc) bc_q(c, q, 1);
+    for (int d = 0; d < 3; ++d)
+      if (on[d]) apply_filter(c, d, q, c->st[5], 5);
+  }
+}
+
+// one step of the loop body of calc_adjoint (computation_adjoint.f90:81-101): time_stepper_adjoint
+// with the frozen direct state q0 and source g, set_boundary_condition_qs(outside_rhs), filters
+void adjoint_loop_step(cruna_ctx *c, double *qs, const double *q0, const double *g, int nt) {
+  const int on[3] = {due(c->cfg.ai_freq[0], nt), due(c->cfg.ai_freq[1], nt), due(c->cfg.ai_freq[2], nt)};
+  if (c->filter_fused_ok && !c->force_generic && (on[0] || on[1] || on[2])) {
+    step_adjoint(c, qs, q0, g, c->st[5]);
+    if (c->has_q_bc) bc_qs(c, c->st[5], q0, 1);
+    filter3_fused(c, c->st[5], qs, on);
+  } else {
+    step_adjoint(c, qs, q0, g, qs);
+    if (c->has_q_bc) bc_qs(c, qs, q0, 1);
+    for (int d = 0; d < 3; ++d)
+      if (on[d]) apply_filter(c, d, qs, c->st[5], 5);
+  }
+}
+
+long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
+                        double *J_dev, double *grad_f, double *grad_q0, std::vector<void *> &scratch);
+
+}  // namespace cruna
+
+extern "C" {
+
 // loop body of calc_direct (computation_direct.f90:64-107); traj is a device pointer or NULL
 static int run_direct_impl(cruna_ctx *c, double *q, int nt0, int nsteps, double *traj, bool traj_host) {
   for (int s = 1; s <= nsteps; ++s) {
     const int nt = nt0 + s;
-    const int on[3] = {due(c->cfg.di_freq[0], nt), due(c->cfg.di_freq[1], nt), due(c->cfg.di_freq[2], nt)};
-    if (c->filter_fused_ok && !c->force_generic && (on[0] || on[1] || on[2])) {
-      step_direct(c, q, c->st[5]);
-      if (c->has_q_bc) bc_q(c, c->st[5], 1);                      // :82
-      filter3_fused(c, c->st[5], q, on);                          // :85-95
-    } else {
-      step_direct(c, q, q);
-      if (c->has_q_bc) bc_q(c, q, 1);                             // :82
-      for (int d = 0; d < 3; ++d)
-        if (on[d]) apply_filter(c, d, q, c->st[5], 5);            // :85-95
-    }
+    direct_loop_step(c, q, nt);
     if (traj) {                                                    // :98-100
       double *dst = traj + (long long)(s - 1) * N5(c);
       CRUNA_CUDA_CHECK(cudaMemcpyAsync(dst, q, sizeof(double) * N5(c),
@@ -793,17 +826,7 @@ static int run_adjoint_impl(cruna_ctx *c, double *qs, const double *Q, const dou
       q0 = dq;
       g = G ? stage_in(c, 2, G + off, 5) : nullptr;
     }
-    const int on[3] = {due(c->cfg.ai_freq[0], nt), due(c->cfg.ai_freq[1], nt), due(c->cfg.ai_freq[2], nt)};
-    if (c->filter_fused_ok && !c->force_generic && (on[0] || on[1] || on[2])) {
-      step_adjoint(c, qs, q0, g, c->st[5]);                       // :81
-      if (c->has_q_bc) bc_qs(c, c->st[5], q0, 1);                  // :88
-      filter3_fused(c, c->st[5], qs, on);                          // :91-101
-    } else {
-      step_adjoint(c, qs, q0, g, qs);                             // :81
-      if (c->has_q_bc) bc_qs(c, qs, q0, 1);                        // :88
-      for (int d = 0; d < 3; ++d)
-        if (on[d]) apply_filter(c, d, qs, c->st[5], 5);           // :91-101
-    }
+    adjoint_loop_step(c, qs, q0, g, nt);
     if (c->cfg.check_every > 0 && nt % c->cfg.check_every == 0) {
       int f = check_state(c, qs);
       if (f & 1) fail(c, CRUNA_ERR_STATE, "adjoint state not finite at step " + std::to_string(nt));
@@ -828,6 +851,59 @@ int cruna_run_adjoint(cruna_ctx *c, double *qs_io, const double *Q_traj, const d
     int rc = run_adjoint_impl(c, dqs, Q_traj, g_traj, nt_end, nsteps, true);
     if (rc) return rc;
     stage_out(c, qs_io, dqs, 5);
+    return CRUNA_OK;
+  });
+}
+
+static int gradient_common(cruna_ctx *c, const double *q0_dev, int nsteps, int nsnap, const cruna_objective *obj,
+                           double *J, double *gf_dev, double *gq_dev, int64_t *direct_steps) {
+  if (!q0_dev || !obj || !J || nsteps < 1 || nsnap < 1) fail(c, CRUNA_ERR_ARG, "bad arguments to cruna_gradient");
+  if (obj->kind != CRUNA_OBJ_PLANE_P2 && obj->kind != CRUNA_OBJ_KINETIC_ENERGY)
+    fail(c, CRUNA_ERR_ARG, "unknown objective kind");
+  if (obj->kind == CRUNA_OBJ_PLANE_P2) {
+    if (obj->normal < 1 || obj->normal > 3) fail(c, CRUNA_ERR_ARG, "objective plane normal must be 1..3");
+    if (obj->index < 1 || obj->index > c->cfg.n[obj->normal - 1])
+      fail(c, CRUNA_ERR_ARG, "objective plane index outside the grid");
+  }
+  std::vector<void *> scratch;
+  double *Jd = nullptr;
+  long long adv = 0;
+  try {
+    void *p = nullptr;
+    CRUNA_CUDA_CHECK(cudaMalloc(&p, sizeof(double)));
+    scratch.push_back(p);
+    Jd = static_cast<double *>(p);
+    adv = gradient_impl(c, q0_dev, nsteps, nsnap, obj, Jd, gf_dev, gq_dev, scratch);
+    CRUNA_CUDA_CHECK(cudaMemcpyAsync(J, Jd, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  } catch (...) {
+    cudaStreamSynchronize(c->stream);
+    for (void *q : scratch) cudaFree(q);
+    throw;
+  }
+  for (void *q : scratch) cudaFree(q);
+  if (direct_steps) *direct_steps = adv;
+  return CRUNA_OK;
+}
+
+int cruna_gradient_dev(cruna_ctx *c, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
+                       double *J, double *grad_f, double *grad_q0, int64_t *direct_steps) {
+  return guarded(c, [&]() -> int {
+    return gradient_common(c, q0, nsteps, nsnap, obj, J, grad_f, grad_q0, direct_steps);
+  });
+}
+
+int cruna_gradient(cruna_ctx *c, const double *q0, int nsteps, int nsnap, const cruna_objective *obj, double *J,
+                   double *grad_f, double *grad_q0, int64_t *direct_steps) {
+  return guarded(c, [&]() -> int {
+    if (!q0) fail(c, CRUNA_ERR_ARG, "null q0");
+    double *dq0 = stage_in(c, 0, q0, 5);
+    double *dgf = grad_f ? stage_in(c, 1, nullptr, 5) : nullptr;
+    double *dgq = grad_q0 ? stage_in(c, 2, nullptr, 5) : nullptr;
+    int rc = gradient_common(c, dq0, nsteps, nsnap, obj, J, dgf, dgq, direct_steps);
+    if (rc) return rc;
+    if (grad_f) stage_out(c, grad_f, dgf, 5);
+    if (grad_q0) stage_out(c, grad_q0, dgq, 5);
     return CRUNA_OK;
   });
 }

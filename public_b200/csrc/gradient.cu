@@ -1,0 +1,278 @@
+// Gradient of an objective through the direct and adjoint loops with binomial checkpointing in HBM.
+//
+// CRUNA's optimisation loop (src/main/cruna.f90:78-179) runs calc_direct, calc_objective,
+// calc_adjoint with calc_objective_g as the adjoint source, then calc_grad; the direct trajectory is
+// kept whole in memory Q(:,:,:,:,nt) (src/data/data_rhs.f90:25) or spilled per time subset to HDF5
+// (computation_direct.f90:131, computation_adjoint.f90:58).  Here the trajectory is recomputed from
+// a few snapshots kept in HBM: rev(a, b, s) produces Q(b) .. Q(a+1) in reverse order from the
+// snapshot Q(a) with s free snapshots -- advance to a + k, store, reverse the right part with s - 1
+// snapshots, run the adjoint step at the snapshot, reverse the left part with s snapshots.  k is
+// chosen by a dynamic programme restricted to the binomial bounds (with t the least number of sweeps
+// such that M(s, t) = C(s+1+t, t) - 1 >= n states, the right part holds at most M(s-1, t) and the left
+// part at most M(s, t-1) states), which gives the minimal number of recomputed direct steps.
+//
+// Objectives (the reference leaves them to each case, src/opt/objective.f90:19-45):
+//   plane_p2:        J = sum_{nt=1..T} dt * sum_plane w (p - p_inf)^2, adjoint source
+//                    g = (0,0,0,0, 2 w (p - p_inf)) on the plane (calc_objective_g)
+//   kinetic_energy:  J = sum dV |rho u|^2 / (2 rho) at t_T, qs(T) = dJ/dq(T)
+// Gradients (calc_grad, force.f90:41-45): dJ/df for a time-constant forcing added to the RHS is the
+// time integral of qs (trapezoid over the adjoint trajectory), dJ/dq0 = qs(0).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "cruna_internal.cuh"
+
+namespace cruna {
+
+namespace {
+
+constexpr int RB = 256;   // reduction block
+constexpr int RG = 592;   // reduction grid (4 x 148): fixed, so sums are deterministic
+
+long long Mst(int s, int t) {
+  // C(s+1+t, t) - 1, saturating
+  double v = 1.0;
+  for (int i = 1; i <= t; ++i) {
+    v = v * (double)(s + 1 + i) / (double)i;
+    if (v > 4e18) return (long long)4e18;
+  }
+  return (long long)std::llround(v) - 1;
+}
+
+// kbest[n*(S+1)+s] = optimal first checkpoint distance for n states and s free snapshots
+void build_schedule(int n, int S, std::vector<int> &kbest, long long &cost_out) {
+  const int W = S + 1;
+  std::vector<long long> cost((size_t)(n + 1) * W, 0);
+  kbest.assign((size_t)(n + 1) * W, 1);
+  for (int s = 0; s <= S; ++s) {
+    for (int m = 1; m <= n; ++m) {
+      long long &c = cost[(size_t)m * W + s];
+      if (s == 0) {
+        c = (long long)m * (m + 1) / 2;
+        continue;
+      }
+      int t = 0;
+      while (Mst(s, t) < m) ++t;
+      const long long lo = std::max<long long>(1, m - Mst(s - 1, t));
+      const long long hi = std::min<long long>(m, Mst(s, t - 1) + 1);
+      long long best = -1;
+      int bk = (int)lo;
+      for (long long k = lo; k <= hi; ++k) {
+        const long long v = k + cost[(size_t)(m - k) * W + (s - 1)] + cost[(size_t)(k - 1) * W + s];
+        if (best < 0 || v < best) {
+          best = v;
+          bk = (int)k;
+        }
+      }
+      c = best;
+      kbest[(size_t)m * W + s] = bk;
+    }
+  }
+  cost_out = cost[(size_t)n * W + S];
+}
+
+// ---- objective kernels (deterministic two-level sums) --------------------------------------------
+__global__ void k_plane_obj(Grid g, int normal, int index, double w, double p_inf, const double *q, double *gsrc,
+                            double *partial) {
+  __shared__ double sh[RB];
+  const long long n1 = g.n1, n2 = g.n2, n3 = g.n3;
+  const long long na = normal == 0 ? n2 : n1, nb = normal == 2 ? n2 : n3;
+  const long long cnt = na * nb;
+  double acc = 0.0;
+  for (long long t = blockIdx.x * (long long)RB + threadIdx.x; t < cnt; t += (long long)RG * RB) {
+    const long long a = t % na, b = t / na;
+    long long i, j, k;
+    if (normal == 0) { i = index; j = a; k = b; }
+    else if (normal == 1) { i = a; j = index; k = b; }
+    else { i = a; j = b; k = index; }
+    const long long p = i + n1 * (j + n2 * k);
+    const double dp = q[p + 4 * g.N] - p_inf;
+    acc += w * dp * dp;
+    gsrc[p + 4 * g.N] = 2.0 * w * dp;
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = RB / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+__global__ void k_ke_obj(Grid g, double dV, const double *q, double *qs_out, double *partial) {
+  __shared__ double sh[RB];
+  double acc = 0.0;
+  const long long N = g.N;
+  for (long long p = blockIdx.x * (long long)RB + threadIdx.x; p < N; p += (long long)RG * RB) {
+    const double r = q[p], mu = q[p + N], mv = q[p + 2 * N], mw = q[p + 3 * N];
+    acc += dV * 0.5 * (mu * mu + mv * mv + mw * mw) / r;
+    if (qs_out) {
+      const double u = mu / r, v = mv / r, w = mw / r;
+      qs_out[p] = dV * (-0.5 * (u * u + v * v + w * w));
+      qs_out[p + N] = dV * u;
+      qs_out[p + 2 * N] = dV * v;
+      qs_out[p + 3 * N] = dV * w;
+      qs_out[p + 4 * N] = 0.0;
+    }
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = RB / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+__global__ void k_sum_partials(const double *partial, int n, double *out, double scale, int accumulate) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += partial[i];
+    out[0] = accumulate ? out[0] + scale * s : scale * s;
+  }
+}
+
+__global__ void k_axpy(long long M, double a, const double *x, double *y, int overwrite) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < M; p += (long long)gridDim.x * blockDim.x)
+    y[p] = overwrite ? a * x[p] : y[p] + a * x[p];
+}
+
+}  // namespace
+
+struct GradientRun {
+  cruna_ctx *c;
+  int nsteps;
+  const cruna_objective *obj;
+  std::vector<int> kbest;
+  int S;
+  double *work;                    // current direct state
+  std::vector<double *> slots;     // snapshot buffers
+  std::vector<int> slot_step;      // step held by a slot, -1 free
+  double *qs, *gsrc, *gf, *J, *partial;
+  long long advanced = 0;
+  void (*direct_step)(cruna_ctx *, double *, int);
+  void (*adjoint_step)(cruna_ctx *, double *, const double *, const double *, int);
+
+  long long M5() const { return c->g.N * 5; }
+  int slot_of(int step) const {
+    for (size_t i = 0; i < slots.size(); ++i)
+      if (slot_step[i] == step) return (int)i;
+    return -1;
+  }
+  int take(int step) {
+    for (size_t i = 0; i < slots.size(); ++i)
+      if (slot_step[i] < 0) {
+        slot_step[i] = step;
+        return (int)i;
+      }
+    throw std::runtime_error("checkpoint schedule ran out of snapshots");
+  }
+  void copy(double *dst, const double *src) { copy_state(c, dst, src, 5); }
+  void advance(int a, int b) {
+    for (int nt = a + 1; nt <= b; ++nt) {
+      direct_step(c, work, nt);
+      ++advanced;
+    }
+  }
+  void axpy(double a, const double *x, double *y, bool overwrite) {
+    k_axpy<<<(int)std::min<long long>((M5() + 255) / 256, 148LL * 32), 256, 0, c->stream>>>(M5(), a, x, y,
+                                                                                             overwrite ? 1 : 0);
+    CRUNA_LAUNCH_CHECK(c);
+  }
+  // adjoint step nt on the direct state Q(nt) (computation_adjoint.f90:66-108)
+  void adjoint(int nt, const double *qnt) {
+    const double dt = c->cfg.dt;
+    const bool plane = obj->kind == CRUNA_OBJ_PLANE_P2;
+    if (nt == nsteps) {
+      if (obj->kind == CRUNA_OBJ_KINETIC_ENERGY) {
+        double dV = 1.0;
+        for (int d = 0; d < 3; ++d)
+          if (c->cfg.n[d] > 1) dV *= c->dx[d];
+        k_ke_obj<<<RG, RB, 0, c->stream>>>(c->g, dV, qnt, qs, partial);
+        CRUNA_LAUNCH_CHECK(c);
+        k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, 1.0, 0);
+        CRUNA_LAUNCH_CHECK(c);
+      }
+      if (gf) axpy(0.5 * dt, qs, gf, true);
+    }
+    if (plane) {
+      const int nd = obj->normal - 1;
+      double w = 1.0;
+      for (int d = 0; d < 3; ++d)
+        if (d != nd && c->cfg.n[d] > 1) w *= c->dx[d];
+      k_plane_obj<<<RG, RB, 0, c->stream>>>(c->g, nd, obj->index - 1, w, obj->p_inf, qnt, gsrc, partial);
+      CRUNA_LAUNCH_CHECK(c);
+      k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, dt, 1);
+      CRUNA_LAUNCH_CHECK(c);
+    }
+    adjoint_step(c, qs, qnt, plane ? gsrc : nullptr, nt);
+    if (gf) axpy(nt - 1 > 0 ? dt : 0.5 * dt, qs, gf, false);
+  }
+  void rev(int a, int b, int s) {
+    const int n = b - a;
+    if (n <= 0) return;
+    const int sa = slot_of(a);
+    if (s == 0) {
+      for (int nt = b; nt > a; --nt) {
+        copy(work, slots[sa]);
+        advance(a, nt);
+        adjoint(nt, work);
+      }
+      return;
+    }
+    const int k = kbest[(size_t)n * (S + 1) + s];
+    const int m = a + k;
+    copy(work, slots[sa]);
+    advance(a, m);
+    const int sm = take(m);
+    copy(slots[sm], work);
+    rev(m, b, s - 1);
+    adjoint(m, slots[sm]);
+    slot_step[sm] = -1;
+    rev(a, m - 1, s);
+  }
+};
+
+// direct / adjoint loop bodies shared with the run loops (capi.cu)
+void direct_loop_step(cruna_ctx *c, double *q, int nt);
+void adjoint_loop_step(cruna_ctx *c, double *qs, const double *q0, const double *g, int nt);
+
+long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
+                        double *J_dev, double *grad_f, double *grad_q0, std::vector<void *> &scratch) {
+  GradientRun g;
+  g.c = c;
+  g.nsteps = nsteps;
+  g.obj = obj;
+  g.S = std::min(nsnap - 1, nsteps);
+  long long cost = 0;
+  build_schedule(nsteps, g.S, g.kbest, cost);
+  const size_t bytes = sizeof(double) * (size_t)c->g.N * 5;
+  auto alloc = [&](size_t b) {
+    void *p = nullptr;
+    CRUNA_CUDA_CHECK(cudaMalloc(&p, b));
+    scratch.push_back(p);
+    return static_cast<double *>(p);
+  };
+  g.work = alloc(bytes);
+  g.slots.resize(g.S + 1);
+  g.slot_step.assign(g.S + 1, -1);
+  for (int i = 0; i <= g.S; ++i) g.slots[i] = alloc(bytes);
+  g.qs = alloc(bytes);
+  g.gsrc = alloc(bytes);
+  g.partial = alloc(sizeof(double) * (RG + 1));
+  g.J = J_dev;
+  g.gf = grad_f;
+  CRUNA_CUDA_CHECK(cudaMemsetAsync(g.qs, 0, bytes, c->stream));
+  CRUNA_CUDA_CHECK(cudaMemsetAsync(g.gsrc, 0, bytes, c->stream));
+  CRUNA_CUDA_CHECK(cudaMemsetAsync(J_dev, 0, sizeof(double), c->stream));
+  g.direct_step = direct_loop_step;
+  g.adjoint_step = adjoint_loop_step;
+  g.slot_step[0] = 0;
+  copy_state(c, g.slots[0], q0, 5);
+  g.rev(0, nsteps, g.S);
+  if (grad_q0) copy_state(c, grad_q0, g.qs, 5);
+  return g.advanced;
+}
+
+}  // namespace cruna

@@ -149,3 +149,66 @@ def test_cpu_twin_matches_oracle():
     cpu_twin.run(s, qc, qsc, 2, 2)
     assert max(O.rel_l2(qc[..., v], q[..., v]) for v in range(5)) < 1e-12
     assert max(O.rel_l2(qsc[..., v], qs[..., v]) for v in range(5)) < 1e-12
+
+
+def test_checkpoint_schedule_order_memory_and_optimality():
+    """Binomial checkpointing: adjoint steps T..1 each once, never more than `slots` snapshots alive,
+    store-all when slots > steps, and the advanced-step count equals the exhaustive minimum."""
+    import functools
+
+    @functools.lru_cache(None)
+    def exhaustive(n, s):
+        if n <= 0:
+            return 0
+        if s == 0:
+            return n * (n + 1) // 2
+        return min(k + exhaustive(n - k, s - 1) + exhaustive(k - 1, s) for k in range(1, n + 1))
+
+    for steps in range(1, 41):
+        for slots in range(1, 7):
+            acts, adv = O.treeverse_schedule(steps, slots)
+            assert [a[1] for a in acts if a[0] == "adjoint"] == list(range(steps, 0, -1))
+            live = mx = 1
+            for a in acts:
+                if a[0] == "store":
+                    live += 1
+                    mx = max(mx, live)
+                elif a[0] == "free":
+                    live -= 1
+            assert mx <= slots
+            assert adv == exhaustive(steps, min(slots - 1, steps))
+    assert O.treeverse_schedule(25, 26)[1] == 25
+
+
+def test_continuous_adjoint_gradient_plumbing_single_step():
+    """Sign and assembly of dJ/dq0 (final-time kinetic energy) with CRUNA's continuous adjoint
+    (ns_rho_rhou_p.f90:257-536) on one small step, where the continuous adjoint's O(dt^2) deviation
+    from the discrete map is negligible."""
+    n = (12, 12, 12)
+    q0 = cases.smooth_random_state(n, seed=21, p0=1.0, rho0=1.0, amp=0.05, x1=(1.0, 1.0, 1.0))
+    cfg = O.Config(n=n, diff=("o8_e_c_p",) * 3, dt=2e-5, mu0=0.0, R=1.0, W=1.0, T0=1.0)
+    S = O.Solver(cfg)
+    J, gf, gq = O.gradient_store_all(S, q0, 1, {"kind": "kinetic_energy"})
+    for k in range(3):
+        d = cases.smooth_random_state(n, seed=40 + k, p0=0.0, rho0=0.0, amp=0.01)
+        eps = 1e-4
+        fd = (O.objective_kinetic_energy(cfg, S.calc_direct(q0 + eps * d, 1))[0]
+              - O.objective_kinetic_energy(cfg, S.calc_direct(q0 - eps * d, 1))[0]) / (2 * eps)
+        assert abs(fd - float(np.sum(gq * d))) < 1e-3 * float(np.linalg.norm(gq) * np.linalg.norm(d))
+
+
+def test_continuous_adjoint_is_not_the_discrete_transpose():
+    """Dot-product test <qs, L dq> vs <rhs_adjoint(qs), dq> with L the linearised direct RHS: CRUNA's
+    continuous adjoint does not satisfy it (it is not the transpose of the discrete operator), which is
+    why an exact finite-difference gradient check needs a discrete adjoint."""
+    n = (12, 12, 12)
+    q = cases.smooth_random_state(n, seed=21, p0=1.0, rho0=1.0, amp=0.05)
+    S = O.Solver(O.Config(n=n, diff=("o8_e_c_p",) * 3, mu0=0.0, R=1.0, W=1.0, T0=1.0))
+    ratios = []
+    for seed in range(2):
+        dq = cases.smooth_random_state(n, seed=50 + seed, p0=0.0, rho0=0.0, amp=1.0)
+        qs = cases.smooth_random_state(n, seed=60 + seed, p0=0.0, rho0=0.0, amp=1.0)
+        eps = 1e-6
+        Ldq = (S.rhs_direct(q + eps * dq) - S.rhs_direct(q - eps * dq)) / (2 * eps)
+        ratios.append(float(np.sum(S.rhs_adjoint(qs, q, np.zeros_like(q)) * dq)) / float(np.sum(qs * Ldq)))
+    assert any(abs(abs(r) - 1.0) > 0.2 for r in ratios), ratios
