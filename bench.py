@@ -123,7 +123,11 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
+            # nvidia-smi needs a moment before its first sample; start timing once it is reporting
+            t0 = time.time()
+            while time.time() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
@@ -209,10 +213,10 @@ def run_ours(args):
     ctx.profile(True)
     launches0 = ctx.launches
     clocks = ClockSampler(local)
+    clocks.start()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks.start()
     for k in range(args.steps):
         nt = args.warmup + k
         ev[k][0].record(stream)

@@ -223,6 +223,29 @@ int cruna_gradient(cruna_ctx *ctx, const double *q0, int nsteps, int nsnap, cons
 int cruna_gradient_dev(cruna_ctx *ctx, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
                        double *J, double *grad_f, double *grad_q0, int64_t *direct_steps);
 
+/* Adjoint used by cruna_gradient: 0 = the reference's continuous inviscid adjoint step
+   (right_hand_side_adjoint_3d, ns_rho_rhou_p.f90:257-536, integrated by time_stepper_adjoint,
+   rk_o4_e.f90:62-105; the default), 1 = the exact discrete adjoint (no counterpart in the reference):
+   the transpose of the direct loop step, so dJ/dq0 and dJ/df are the exact derivatives of the J the
+   direct loop produces.  Mode 1 needs precision CRUNA_FP64; it runs the generic line-operator kernels
+   and keeps about 160 doubles per grid point of device memory. */
+int cruna_set_adjoint_mode(cruna_ctx *ctx, int mode);
+
+/* Discrete adjoint of right_hand_side_direct_3d (ns_rho_rhou_p.f90:31-253; no counterpart in the
+   reference): mu = (d rhs/d q)^T lam at q, through the BC on q, every derivative, the viscous terms,
+   the forcing and the BC on the RHS.  grad_f (may be NULL) is accumulated with (d rhs/d f)^T lam. */
+int cruna_rhs_direct_vjp(cruna_ctx *ctx, const double *q, const double *lam, double *mu, double *grad_f);
+int cruna_rhs_direct_vjp_dev(cruna_ctx *ctx, const double *q, const double *lam, double *mu, double *grad_f);
+
+/* Discrete adjoint of loop step nt of calc_direct (computation_direct.f90:64-107: time_stepper_direct,
+   BC on q outside the RHS, filters when mod(nt, freq) == 0) at its input q0 (no counterpart in the
+   reference): lam0 = (d q1/d q0)^T lam1; grad_f (may be NULL) accumulates (d q1/d f)^T lam1.
+   lam0 may alias lam1. */
+int cruna_step_direct_vjp(cruna_ctx *ctx, const double *q0, const double *lam1, double *lam0, double *grad_f,
+                          int nt);
+int cruna_step_direct_vjp_dev(cruna_ctx *ctx, const double *q0, const double *lam1, double *lam0,
+                              double *grad_f, int nt);
+
 /* State check used by the run loops: returns CRUNA_ERR_STATE if any rho <= 0, p <= 0 or a
    non-finite value is found in q (device pointer). */
 int cruna_check_state_dev(cruna_ctx *ctx, const double *q);

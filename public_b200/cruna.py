@@ -115,6 +115,11 @@ _SIGNATURES = {
     "cruna_profile_enable": (_I, [_P, _I]),
     "cruna_profile_report": (_I, [_P, C.c_char_p, _I]),
     "cruna_rhs_direct_noalloc": (_I, [C.POINTER(_Config), _P, _P, _P, C.c_char_p, _I]),
+    "cruna_set_adjoint_mode": (_I, [_P, _I]),
+    "cruna_rhs_direct_vjp": (_I, [_P, _P, _P, _P, _P]),
+    "cruna_rhs_direct_vjp_dev": (_I, [_P, _P, _P, _P, _P]),
+    "cruna_step_direct_vjp": (_I, [_P, _P, _P, _P, _P, _I]),
+    "cruna_step_direct_vjp_dev": (_I, [_P, _P, _P, _P, _P, _I]),
     "cruna_gradient": (_I, [_P, _P, _I, _I, C.POINTER(Objective), C.POINTER(C.c_double), _P, _P,
                             C.POINTER(C.c_int64)]),
     "cruna_gradient_dev": (_I, [_P, _P, _I, _I, C.POINTER(Objective), C.POINTER(C.c_double), _P, _P,
@@ -411,6 +416,30 @@ class Cruna:
         o.kind = {"plane_p2": 1, "kinetic_energy": 2}[kind]
         o.normal, o.index, o.p_inf = int(normal), int(index), float(p_inf)
         return o
+
+    def set_adjoint_mode(self, mode: int):
+        """0: the reference's continuous adjoint (default); 1: the exact discrete adjoint."""
+        self._check(self.lib.cruna_set_adjoint_mode(self.h, int(mode)))
+
+    def rhs_direct_vjp(self, q, lam, grad_f=None):
+        """(d rhs_direct/d q)^T lam; grad_f (a state array, updated in place) accumulates (d rhs/d f)^T lam."""
+        a, l = self._state(q), self._state(lam)
+        mu = np.empty_like(a, order="F")
+        gf = None if grad_f is None else self._state(grad_f)
+        self._check(self.lib.cruna_rhs_direct_vjp(self.h, _ptr(a), _ptr(l), _ptr(mu), _ptr(gf)))
+        if grad_f is not None and gf is not grad_f:
+            grad_f[...] = gf
+        return mu
+
+    def step_direct_vjp(self, q0, lam1, nt: int, grad_f=None):
+        """Transpose of direct loop step nt at q0 applied to lam1 (grad_f accumulated in place)."""
+        a, l = self._state(q0), self._state(lam1)
+        out = np.empty_like(a, order="F")
+        gf = None if grad_f is None else self._state(grad_f)
+        self._check(self.lib.cruna_step_direct_vjp(self.h, _ptr(a), _ptr(l), _ptr(out), _ptr(gf), int(nt)))
+        if grad_f is not None and gf is not grad_f:
+            grad_f[...] = gf
+        return out
 
     def gradient(self, q0, nsteps: int, nsnap: int, objective: Objective):
         """J, dJ/df, dJ/dq0 and the number of direct steps executed (binomial checkpointing)."""

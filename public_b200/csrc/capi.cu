@@ -9,6 +9,28 @@
 
 using namespace cruna;
 
+namespace cruna {
+
+double *dalloc(cruna_ctx *c, size_t count) {
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, count * sizeof(double));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw ApiError{CRUNA_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(count * 8) +
+                                        " bytes failed: " + cudaGetErrorString(e)};
+  }
+  c->allocations.push_back(p);
+  return static_cast<double *>(p);
+}
+
+void ensure_generic(cruna_ctx *c) {
+  if (!c->tmp) c->tmp = dalloc(c, (size_t)c->g.N * 60);
+}
+
+bool use_fused(const cruna_ctx *c) { return c->fused_ok && !c->force_generic; }
+
+}  // namespace cruna
+
 namespace {
 
 thread_local std::string g_init_error;
@@ -26,6 +48,9 @@ int guarded(cruna_ctx *c, F &&f) {
     return rc;
   } catch (const Status &s) {
     return s.code;
+  } catch (const ApiError &e) {
+    c->err = e.msg;
+    return e.code;
   } catch (const std::bad_alloc &) {
     c->err = "host allocation failed";
     return CRUNA_ERR_NOMEM;
@@ -38,18 +63,6 @@ int guarded(cruna_ctx *c, F &&f) {
 [[noreturn]] void fail(cruna_ctx *c, int code, const std::string &msg) {
   c->err = msg;
   throw Status{code};
-}
-
-double *dalloc(cruna_ctx *c, size_t count) {
-  void *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, count * sizeof(double));
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    fail(c, CRUNA_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(count * 8) + " bytes failed: " +
-                                 cudaGetErrorString(e));
-  }
-  c->allocations.push_back(p);
-  return static_cast<double *>(p);
 }
 
 template <class T>
@@ -87,17 +100,18 @@ double *stage_in(cruna_ctx *c, int slot, const double *host, int nfields) {
   return c->io[slot];
 }
 
+// grad_f of the host-pointer VJP entry points has its own buffer: io[3] may hold the forcing
+double *stage_gf(cruna_ctx *c, const double *host) {
+  if (!c->vjp_gf) c->vjp_gf = dalloc(c, (size_t)N5(c));
+  CRUNA_CUDA_CHECK(cudaMemcpyAsync(c->vjp_gf, host, sizeof(double) * N5(c), cudaMemcpyHostToDevice, c->stream));
+  return c->vjp_gf;
+}
+
 void stage_out(cruna_ctx *c, double *host, const double *dev, int nfields) {
   CRUNA_CUDA_CHECK(cudaMemcpyAsync(host, dev, sizeof(double) * c->g.N * nfields, cudaMemcpyDeviceToHost,
                                    c->stream));
   CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
 }
-
-void ensure_generic(cruna_ctx *c) {
-  if (!c->tmp) c->tmp = dalloc(c, (size_t)c->g.N * 60);
-}
-
-bool use_fused(const cruna_ctx *c) { return c->fused_ok && !c->force_generic; }
 
 // time_stepper_direct (rk_o4_e.f90:17-58): q1 may alias q0
 void step_direct(cruna_ctx *c, const double *q0, double *q1) {
@@ -286,11 +300,13 @@ int cruna_init(const cruna_config *cfg, const double *bc_table, int nbc, cruna_c
       if (!build_diff_op(cfg->diff[d], cfg->n[d], c->dop[d], hf, err))
         fail(c, CRUNA_ERR_ARG, "direction " + std::to_string(d + 1) + ": " + err);
       attach_factors(c, c->dop[d], hf);
+      c->dhf[d] = hf;
       HostFactors hf2;
       if (!build_filter_op(cfg->filter[d], cfg->n[d], cfg->filter_alpha, cfg->filter_strength, c->fop[d],
                            hf2, err))
         fail(c, CRUNA_ERR_ARG, "direction " + std::to_string(d + 1) + ": " + err);
       attach_factors(c, c->fop[d], hf2);
+      c->fhf[d] = hf2;
     }
     // boundary table (boundary_conditions.f90:461-610: inf -> n, clamp to the block)
     if (nbc < 0 || (nbc > 0 && !bc_table)) fail(c, CRUNA_ERR_ARG, "bad boundary table");
@@ -884,6 +900,58 @@ static int gradient_common(cruna_ctx *c, const double *q0_dev, int nsteps, int n
   for (void *q : scratch) cudaFree(q);
   if (direct_steps) *direct_steps = adv;
   return CRUNA_OK;
+}
+
+int cruna_set_adjoint_mode(cruna_ctx *c, int mode) {
+  return guarded(c, [&]() -> int {
+    if (mode != 0 && mode != 1) fail(c, CRUNA_ERR_ARG, "adjoint mode must be 0 (continuous) or 1 (discrete)");
+    if (mode == 1 && c->cfg.precision != CRUNA_FP64)
+      fail(c, CRUNA_ERR_UNSUPPORTED, "the discrete adjoint needs precision CRUNA_FP64");
+    c->adjoint_mode = mode;
+    return CRUNA_OK;
+  });
+}
+
+int cruna_rhs_direct_vjp_dev(cruna_ctx *c, const double *q, const double *lam, double *mu, double *grad_f) {
+  return guarded(c, [&]() -> int {
+    if (!q || !lam || !mu) fail(c, CRUNA_ERR_ARG, "null pointer");
+    rhs_direct_vjp(c, q, lam, mu, grad_f);
+    return CRUNA_OK;
+  });
+}
+
+int cruna_rhs_direct_vjp(cruna_ctx *c, const double *q, const double *lam, double *mu, double *grad_f) {
+  return guarded(c, [&]() -> int {
+    if (!q || !lam || !mu) fail(c, CRUNA_ERR_ARG, "null pointer");
+    double *dq = stage_in(c, 0, q, 5), *dl = stage_in(c, 1, lam, 5), *dm = stage_in(c, 2, nullptr, 5);
+    double *dg = grad_f ? stage_gf(c, grad_f) : nullptr;
+    rhs_direct_vjp(c, dq, dl, dm, dg);
+    if (dg) stage_out(c, grad_f, dg, 5);
+    stage_out(c, mu, dm, 5);
+    return CRUNA_OK;
+  });
+}
+
+int cruna_step_direct_vjp_dev(cruna_ctx *c, const double *q0, const double *lam1, double *lam0, double *grad_f,
+                              int nt) {
+  return guarded(c, [&]() -> int {
+    if (!q0 || !lam1 || !lam0) fail(c, CRUNA_ERR_ARG, "null pointer");
+    step_direct_vjp(c, q0, lam1, lam0, grad_f, nt);
+    return CRUNA_OK;
+  });
+}
+
+int cruna_step_direct_vjp(cruna_ctx *c, const double *q0, const double *lam1, double *lam0, double *grad_f,
+                          int nt) {
+  return guarded(c, [&]() -> int {
+    if (!q0 || !lam1 || !lam0) fail(c, CRUNA_ERR_ARG, "null pointer");
+    double *dq = stage_in(c, 0, q0, 5), *dl = stage_in(c, 1, lam1, 5), *dm = stage_in(c, 2, nullptr, 5);
+    double *dg = grad_f ? stage_gf(c, grad_f) : nullptr;
+    step_direct_vjp(c, dq, dl, dm, dg, nt);
+    if (dg) stage_out(c, grad_f, dg, 5);
+    stage_out(c, lam0, dm, 5);
+    return CRUNA_OK;
+  });
 }
 
 int cruna_gradient_dev(cruna_ctx *c, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,

@@ -48,9 +48,23 @@ struct LineOp {
 // Host-side copy of the factors (filled by the dgttrf restatement in schemes.cpp).
 struct HostFactors {
   std::vector<double> dl, d, du, du2, fbnorm;
+  std::vector<double> raw_dl, raw_d, raw_du;  // the tridiagonal matrix before dgttrf (for B^T)
   std::vector<int> ipiv;  // 1-based as LAPACK
   double fbrat = 0.0;
   int info = 0;
+};
+
+// Transpose of a line operator (discrete adjoint): out = scale * A^T (B^-T in) where the operator is
+// B^-1 A.  A^T is kept as a band: band[j*(hi-lo+1) + (o-lo)] multiplies in[j+o] (wrapped on
+// periodic lines); sop holds the factors of B^T (B itself when B is symmetric).
+struct LineOpT {
+  int n = 1;
+  int kind = OP_ZERO;   // OP_ZERO, OP_COPY (identity) or OP_STENCIL (band)
+  int periodic = 0;
+  int lo = 0, hi = 0;
+  const double *band = nullptr;
+  int solve = 0;
+  LineOp sop;
 };
 
 struct Grid {
@@ -67,6 +81,12 @@ bool diff_is_periodic(int scheme);
 int lapack_dgttrf(int n, double *dl, double *d, double *du, double *du2, int *ipiv);
 void lapack_dgttrs(int n, const double *dl, const double *d, const double *du, const double *du2,
                    const int *ipiv, double *b);
+
+// error raised inside the library and returned by the extern "C" entry points as (code, message)
+struct ApiError {
+  int code;
+  std::string msg;
+};
 
 struct BCRow {
   int type;
@@ -123,6 +143,15 @@ struct cruna_ctx {
   float *fz32 = nullptr;         // fused-path FP32 intermediates
   double *red = nullptr;         // reduction scratch
   int *flag = nullptr;           // device error flag
+  // discrete adjoint (discrete_adjoint.cu): host factors kept for the transposes, built on first use
+  cruna::HostFactors dhf[3], fhf[3];
+  bool vjp_ready = false;
+  cruna::LineOpT dopT[3], fopT[3];
+  double *vjp_ws = nullptr;        // backward workspace (fields)
+  double *vjp_st[12] = {nullptr};  // state-sized buffers of the transposed step
+  std::vector<double *> vjp_save;  // per boundary row: box values before the row (q, aim / rhs)
+  double *vjp_gf = nullptr;        // staging of grad_f for the host-pointer entry points (io[3] holds f)
+  int adjoint_mode = 0;            // cruna_gradient: 0 continuous (reference), 1 discrete
 };
 
 namespace cruna {
@@ -136,7 +165,9 @@ void apply_diff(cruna_ctx *c, int dir, const double *f1, const double *f2, doubl
 void apply_filter(cruna_ctx *c, int dir, double *q, double *scratch, int nfields);
 
 // RHS / BC / RK (ops.cu, fused.cu)
-void rhs_direct_generic(cruna_ctx *c, const double *q, double *rhs, double *qbc_scratch);
+// bc_mask: 1 applies the BC on q before, 2 the BC on the RHS after (3 = the reference order)
+void rhs_direct_generic(cruna_ctx *c, const double *q, double *rhs, double *qbc_scratch, int bc_mask = 3);
+void generic_forward_gradients(cruna_ctx *c, const double *q);  // primitives, grads, mu, tau into tmp
 void rhs_adjoint_generic(cruna_ctx *c, const double *qs, const double *q, const double *g, double *rhs,
                          double *qsbc_scratch);
 bool fused_supported(const cruna_ctx *c);
@@ -154,6 +185,13 @@ void rk_stage(cruna_ctx *c, int stage, double dt, const double *k, const double 
               double *qnext);
 void copy_state(cruna_ctx *c, double *dst, const double *src, int nfields);
 int check_state(cruna_ctx *c, const double *q);
+double *dalloc(cruna_ctx *c, size_t count);
+void ensure_generic(cruna_ctx *c);
+bool use_fused(const cruna_ctx *c);
+// discrete adjoint (discrete_adjoint.cu)
+void rhs_direct_vjp(cruna_ctx *c, const double *q, const double *lam, double *mu, double *gf_acc);
+void step_direct_vjp(cruna_ctx *c, const double *q0, const double *lam1, double *lam0, double *gf_acc,
+                     int nt);
 void add_fields(cruna_ctx *c, double *dst, const double *src, long long n);
 
 // kernel timing helpers (capi.cu)

@@ -17,6 +17,9 @@
 //   kinetic_energy:  J = sum dV |rho u|^2 / (2 rho) at t_T, qs(T) = dJ/dq(T)
 // Gradients (calc_grad, force.f90:41-45): dJ/df for a time-constant forcing added to the RHS is the
 // time integral of qs (trapezoid over the adjoint trajectory), dJ/dq0 = qs(0).
+// Discrete mode (cruna_set_adjoint_mode 1) replaces the reference's continuous adjoint step by the
+// exact transpose of the direct loop step (discrete_adjoint.cu): J is the same sum over the same
+// states, and dJ/dq0, dJ/df are its exact derivatives.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -150,6 +153,8 @@ struct GradientRun {
   std::vector<double *> slots;     // snapshot buffers
   std::vector<int> slot_step;      // step held by a slot, -1 free
   double *qs, *gsrc, *gf, *J, *partial;
+  double *qN = nullptr;            // discrete mode: the final state Q(nsteps)
+  bool discrete = false;
   long long advanced = 0;
   void (*direct_step)(cruna_ctx *, double *, int);
   void (*adjoint_step)(cruna_ctx *, double *, const double *, const double *, int);
@@ -180,8 +185,50 @@ struct GradientRun {
                                                                                              overwrite ? 1 : 0);
     CRUNA_LAUNCH_CHECK(c);
   }
+  void plane_source(const double *q) {
+    const int nd = obj->normal - 1;
+    double w = 1.0;
+    for (int d = 0; d < 3; ++d)
+      if (d != nd && c->cfg.n[d] > 1) w *= c->dx[d];
+    k_plane_obj<<<RG, RB, 0, c->stream>>>(c->g, nd, obj->index - 1, w, obj->p_inf, q, gsrc, partial);
+    CRUNA_LAUNCH_CHECK(c);
+    k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, c->cfg.dt, 1);
+    CRUNA_LAUNCH_CHECK(c);
+  }
+  // discrete mode: the state Q(nt) is the input of step nt + 1, whose transpose maps the cotangent of
+  // Q(nt + 1) to that of Q(nt); the objective's own term at Q(nt) is added after it
+  void adjoint_discrete(int nt, const double *qnt) {
+    const double dt = c->cfg.dt;
+    const bool plane = obj->kind == CRUNA_OBJ_PLANE_P2;
+    if (nt == nsteps - 1) {
+      copy(qN, qnt);
+      direct_step(c, qN, nsteps);
+      ++advanced;
+      if (plane) {
+        plane_source(qN);
+        axpy(dt, gsrc, qs, true);
+      } else {
+        double dV = 1.0;
+        for (int d = 0; d < 3; ++d)
+          if (c->cfg.n[d] > 1) dV *= c->dx[d];
+        k_ke_obj<<<RG, RB, 0, c->stream>>>(c->g, dV, qN, qs, partial);
+        CRUNA_LAUNCH_CHECK(c);
+        k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, 1.0, 0);
+        CRUNA_LAUNCH_CHECK(c);
+      }
+    }
+    step_direct_vjp(c, qnt, qs, qs, gf, nt + 1);
+    if (plane && nt >= 1) {
+      plane_source(qnt);
+      axpy(dt, gsrc, qs, false);
+    }
+  }
   // adjoint step nt on the direct state Q(nt) (computation_adjoint.f90:66-108)
   void adjoint(int nt, const double *qnt) {
+    if (discrete) {
+      adjoint_discrete(nt, qnt);
+      return;
+    }
     const double dt = c->cfg.dt;
     const bool plane = obj->kind == CRUNA_OBJ_PLANE_P2;
     if (nt == nsteps) {
@@ -244,9 +291,12 @@ long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, c
   g.c = c;
   g.nsteps = nsteps;
   g.obj = obj;
-  g.S = std::min(nsnap - 1, nsteps);
+  g.discrete = c->adjoint_mode == 1;
+  // discrete mode reverses the step inputs Q(nsteps-1) .. Q(0); the continuous one Q(nsteps) .. Q(1)
+  const int span = g.discrete ? nsteps - 1 : nsteps;
+  g.S = std::min(nsnap - 1, std::max(span, 0));
   long long cost = 0;
-  build_schedule(nsteps, g.S, g.kbest, cost);
+  build_schedule(span, g.S, g.kbest, cost);
   const size_t bytes = sizeof(double) * (size_t)c->g.N * 5;
   auto alloc = [&](size_t b) {
     void *p = nullptr;
@@ -270,7 +320,14 @@ long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, c
   g.adjoint_step = adjoint_loop_step;
   g.slot_step[0] = 0;
   copy_state(c, g.slots[0], q0, 5);
-  g.rev(0, nsteps, g.S);
+  if (g.discrete) {
+    g.qN = alloc(bytes);
+    if (grad_f) CRUNA_CUDA_CHECK(cudaMemsetAsync(grad_f, 0, bytes, c->stream));
+    g.rev(0, span, g.S);
+    g.adjoint(0, g.slots[0]);
+  } else {
+    g.rev(0, nsteps, g.S);
+  }
   if (grad_q0) copy_state(c, grad_q0, g.qs, 5);
   return g.advanced;
 }

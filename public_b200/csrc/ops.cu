@@ -5,82 +5,11 @@
 #include <stdexcept>
 #include <string>
 
+#include "bc_point.cuh"
 #include "cruna_internal.cuh"
+#include "ops_common.cuh"
 
 namespace cruna {
-
-constexpr int kThreads = 256;
-
-static inline int nblocks(long long work, int threads = kThreads) {
-  long long b = (work + threads - 1) / threads;
-  return (int)(b < 1 ? 1 : b);
-}
-
-// ------------------------------------------------------------------------------------------------
-// line operators
-// ------------------------------------------------------------------------------------------------
-__device__ __forceinline__ void line_geom(const Grid &g, int dir, long long p, long long &base,
-                                          long long &stride, int &i) {
-  // p is a point index inside one field; returns the line base offset, stride and position
-  const long long n1 = g.n1, n12 = (long long)g.n1 * g.n2;
-  const long long ii = p % n1, jj = (p / n1) % g.n2, kk = p / n12;
-  if (dir == 0) { i = (int)ii; stride = 1; base = p - ii; }
-  else if (dir == 1) { i = (int)jj; stride = n1; base = p - jj * n1; }
-  else { i = (int)kk; stride = n12; base = p - kk * n12; }
-}
-
-__device__ __forceinline__ double ldv(const double *f1, const double *f2, long long idx) {
-  return f2 ? f1[idx] * f2[idx] : f1[idx];
-}
-
-// explicit part of the operator at position i of the line starting at f + base
-__device__ double explicit_part(const LineOp &op, const double *f1, const double *f2, long long base,
-                                long long s, int i) {
-  const int n = op.n;
-  if (op.kind == OP_ZERO) return 0.0;
-  if (op.kind == OP_COPY) return ldv(f1, f2, base + i * s);
-  if (op.periodic) {
-    if (op.antisym) {
-      double t = 0.0;
-      for (int m = 1; m <= op.r; ++m) {
-        int ip = (i + m) % n, im = ((i - m) % n + n) % n;
-        double d = ldv(f1, f2, base + ip * s) - ldv(f1, f2, base + im * s);
-        t = (m == 1) ? op.c[1] * d : t + op.c[m] * d;
-      }
-      return t;
-    }
-    double t = op.c[0] * ldv(f1, f2, base + i * s);
-    for (int m = 1; m <= op.r; ++m) {
-      int ip = (i + m) % n, im = ((i - m) % n + n) % n;
-      t = t + op.c[m] * (ldv(f1, f2, base + ip * s) + ldv(f1, f2, base + im * s));
-    }
-    return t;
-  }
-  if (i >= op.nb && i < n - op.nb) {
-    if (op.antisym) {
-      double t = 0.0;
-      for (int m = 1; m <= op.r; ++m) {
-        double d = ldv(f1, f2, base + (i + m) * s) - ldv(f1, f2, base + (i - m) * s);
-        t = (m == 1) ? op.c[1] * d : t + op.c[m] * d;
-      }
-      return t;
-    }
-    double t = op.c[0] * ldv(f1, f2, base + i * s);
-    for (int m = 1; m <= op.r; ++m)
-      t = t + op.c[m] * (ldv(f1, f2, base + (i + m) * s) + ldv(f1, f2, base + (i - m) * s));
-    return t;
-  }
-  const bool start = i < op.nb;
-  const int row = start ? i : n - 1 - i;
-  if (op.keep_ends && row == 0) return ldv(f1, f2, base + i * s);
-  double t = 0.0;
-  for (int m = 0; m < op.bw; ++m) {
-    const int j = start ? m : n - 1 - m;
-    t = (m == 0) ? op.brow[row][0] * ldv(f1, f2, base + j * s)
-                 : t + op.brow[row][m] * ldv(f1, f2, base + j * s);
-  }
-  return (op.antisym && !start) ? -t : t;
-}
 
 __global__ void k_line_stencil(LineOp op, Grid g, int dir, const double *__restrict__ f1,
                                const double *__restrict__ f2, double *__restrict__ out, double scale,
@@ -94,13 +23,7 @@ __global__ void k_line_stencil(LineOp op, Grid g, int dir, const double *__restr
     line_geom(g, dir, p, base, s, i);
     const double *a = f1 + fld * g.N;
     const double *b = f2 ? f2 + fld * g.N : nullptr;
-    double v = explicit_part(op, a, b, base, s, i);
-    if (op.kind == OP_STENCIL && op.antisym) v = v * scale;
-    if (op.blend > 0.0) {
-      const double q = ldv(a, b, p);
-      v = q - op.blend * (q - v);
-    }
-    out[t] = sign * v;
+    out[t] = sign * line_point(op, a, b, base, s, i, scale);
   }
 }
 
@@ -183,34 +106,8 @@ void apply_filter(cruna_ctx *c, int dir, double *q, double *scratch, int nfields
 }
 
 // ------------------------------------------------------------------------------------------------
-// sponge shape on the fly: phi = (((sx*sym)*syp)*szm)*szp, shape = amp*(1 - phi)
-// (src/boundaries/shape_functions.f90:104-145)
-// ------------------------------------------------------------------------------------------------
-__device__ __forceinline__ double sponge_at(const SpongeDev &sp, const Grid &g, long long p) {
-  const long long i = p % g.n1, j = (p / g.n1) % g.n2, k = p / ((long long)g.n1 * g.n2);
-  double phi = sp.sx[i] * sp.sym[j];
-  phi = phi * sp.syp[j];
-  phi = phi * sp.szm[k];
-  phi = phi * sp.szp[k];
-  return sp.amp * (1.0 - phi);
-}
-
-// ------------------------------------------------------------------------------------------------
 // boundary kernels
 // ------------------------------------------------------------------------------------------------
-struct Box {
-  int is, ie, js, je, ks, ke;
-  __host__ __device__ long long count() const { return (long long)(ie - is + 1) * (je - js + 1) * (ke - ks + 1); }
-};
-
-__device__ __forceinline__ long long box_point(const Box &b, const Grid &g, long long t, int &i, int &j,
-                                               int &k) {
-  const int ni = b.ie - b.is + 1, nj = b.je - b.js + 1;
-  i = b.is + (int)(t % ni);
-  j = b.js + (int)((t / ni) % nj);
-  k = b.ks + (int)(t / ((long long)ni * nj));
-  return i + (long long)g.n1 * (j + (long long)g.n2 * k);
-}
 
 // characteristic_q_k1d (src/boundaries/nonreflecting.f90:46-137) -- aim from `aim` at p + aim_off
 __global__ void k_char_q(Box b, Grid g, double k1, double k2, double k3, double gamma, double *q,
@@ -221,37 +118,13 @@ __global__ void k_char_q(Box b, Grid g, double k1, double k2, double k3, double 
     int i, j, k;
     const long long p = box_point(b, g, t, i, j, k);
     const long long N = g.N, pa = p + aim_off;
-    const double r = q[p], u0 = q[p + N] / r, u1 = q[p + 2 * N] / r, u2 = q[p + 3 * N] / r, pp = q[p + 4 * N];
-    const double c = sqrt(gamma * q[p + 4 * N] / q[p]);
-    const double ar = aim[pa];
-    const double d0 = ar - r;
-    const double d1 = aim[pa + N] / ar - u0;
-    const double d2 = aim[pa + 2 * N] / ar - u1;
-    const double d3 = aim[pa + 3 * N] / ar - u2;
-    const double d4 = aim[pa + 4 * N] - pp;
-    const double kx = -k1, ky = -k2, kz = -k3;
-    const double c2 = c * c;
-    double R1 = kx * d0 + kz * d2 - ky * d3 - kx * d4 / c2;
-    double R2 = ky * d0 - kz * d1 + kx * d3 - ky * d4 / c2;
-    double R3 = kz * d0 + ky * d1 - kx * d2 - kz * d4 / c2;
-    double R4 = kx * d1 + ky * d2 + kz * d3 + d4 / (r * c);
-    double R5 = -kx * d1 - ky * d2 - kz * d3 + d4 / (r * c);
-    const double lamS = kx * u0 + ky * u1 + kz * u2;
-    const double lamP = lamS + c, lamM = lamS - c;
-    if (lamS < 0.0) { R1 = 0.0; R2 = 0.0; R3 = 0.0; }
-    if (lamP < 0.0) R4 = 0.0;
-    if (lamM < 0.0) R5 = 0.0;
-    const double e1 = kx * R1 + ky * R2 + kz * R3 + r / (2.0 * c) * R4 + r / (2.0 * c) * R5;
-    const double e2 = -kz * R2 + ky * R3 + 0.5 * kx * R4 - 0.5 * kx * R5;
-    const double e3 = kz * R1 - kx * R3 + 0.5 * ky * R4 - 0.5 * ky * R5;
-    const double e4 = -ky * R1 + kx * R2 + 0.5 * kz * R4 - 0.5 * kz * R5;
-    const double e5 = +0.5 * r * c * R4 + 0.5 * r * c * R5;
-    const double rn = r + e1;
-    q[p] = rn;
-    q[p + N] = rn * (u0 + e2);
-    q[p + 2 * N] = rn * (u1 + e3);
-    q[p + 3 * N] = rn * (u2 + e4);
-    q[p + 4 * N] = pp + e5;
+    double qv[5], av[5], out[5];
+    for (int v = 0; v < 5; ++v) {
+      qv[v] = q[p + v * N];
+      av[v] = aim[pa + v * N];
+    }
+    char_q_point(qv, av, k1, k2, k3, gamma, out);
+    for (int v = 0; v < 5; ++v) q[p + v * N] = out[v];
   }
 }
 
@@ -310,40 +183,14 @@ __global__ void k_char_rhs(Box b, Grid g, double k1, double k2, double k3, doubl
     int i, j, k;
     const long long p = box_point(b, g, t, i, j, k);
     const long long N = g.N;
-    const double inv_dt = 1.0 / dt;
-    const double r = q[p], u0 = q[p + N] / r, u1 = q[p + 2 * N] / r, u2 = q[p + 3 * N] / r;
-    const double c = sqrt(gamma * q[p + 4 * N] / q[p]);
-    const double ar = aim[p];
-    double d0 = ar - r, d1 = aim[p + N] / ar - u0, d2 = aim[p + 2 * N] / ar - u1,
-           d3 = aim[p + 3 * N] / ar - u2, d4 = aim[p + 4 * N] - q[p + 4 * N];
-    const double tmp = dt / r;
-    d0 = d0 + rhs[p] * dt;
-    d1 = d1 + rhs[p + N] * tmp;
-    d2 = d2 + rhs[p + 2 * N] * tmp;
-    d3 = d3 + rhs[p + 3 * N] * tmp;
-    d4 = d4 + rhs[p + 4 * N] * dt;
-    const double kx = -k1, ky = -k2, kz = -k3, c2 = c * c;
-    double R1 = kx * d0 + kz * d2 - ky * d3 - kx * d4 / c2;
-    double R2 = ky * d0 - kz * d1 + kx * d3 - ky * d4 / c2;
-    double R3 = kz * d0 + ky * d1 - kx * d2 - kz * d4 / c2;
-    double R4 = kx * d1 + ky * d2 + kz * d3 + d4 / (r * c);
-    double R5 = -kx * d1 - ky * d2 - kz * d3 + d4 / (r * c);
-    const double lamS = kx * u0 + ky * u1 + kz * u2;
-    if (lamS < 0.0) { R1 = 0.0; R2 = 0.0; R3 = 0.0; }
-    if (lamS + c < 0.0) R4 = 0.0;
-    if (lamS - c < 0.0) R5 = 0.0;
-    const double e1 = kx * R1 + ky * R2 + kz * R3 + r / (2.0 * c) * R4 + r / (2.0 * c) * R5;
-    const double e2 = -kz * R2 + ky * R3 + 0.5 * kx * R4 - 0.5 * kx * R5;
-    const double e3 = kz * R1 - kx * R3 + 0.5 * ky * R4 - 0.5 * ky * R5;
-    const double e4 = -ky * R1 + kx * R2 + 0.5 * kz * R4 - 0.5 * kz * R5;
-    const double e5 = +0.5 * r * c * R4 + 0.5 * r * c * R5;
-    const double rn = r + e1;
-    rhs[p] = e1 * inv_dt;
-    const double t2 = inv_dt * rn;
-    rhs[p + N] = e2 * t2;
-    rhs[p + 2 * N] = e3 * t2;
-    rhs[p + 3 * N] = e4 * t2;
-    rhs[p + 4 * N] = e5 * inv_dt;
+    double rv[5], qv[5], av[5], out[5];
+    for (int v = 0; v < 5; ++v) {
+      rv[v] = rhs[p + v * N];
+      qv[v] = q[p + v * N];
+      av[v] = aim[p + v * N];
+    }
+    char_rhs_point(rv, qv, av, k1, k2, k3, gamma, dt, out);
+    for (int v = 0; v < 5; ++v) rhs[p + v * N] = out[v];
   }
 }
 
@@ -387,12 +234,6 @@ __global__ void k_sponge(int mode, Grid g, SpongeDev sp, double gamma, double *a
       a[p + 4 * N] += sh * s4;
     }
   }
-}
-
-static Box box_of(const BCRow &r) { return Box{r.is, r.ie, r.js, r.je, r.ks, r.ke}; }
-
-static long long offset_of(const cruna_ctx *c, const int sh[3]) {
-  return sh[0] + (long long)c->g.n1 * (sh[1] + (long long)c->g.n2 * sh[2]);
 }
 
 void bc_q(cruna_ctx *c, double *q, int /*outside*/) {
@@ -543,18 +384,6 @@ int check_state(cruna_ctx *c, const double *q) {
 // generic direct RHS: the call sequence of right_hand_side_direct_3d (ns_rho_rhou_p.f90:31-253)
 // with the point-wise work fused into a few kernels
 // ------------------------------------------------------------------------------------------------
-enum GenericField {
-  F_U1, F_U2, F_U3, F_T,
-  F_UX, F_UY, F_UZ, F_VX, F_VY, F_VZ, F_WX, F_WY, F_WZ, F_TX, F_TY, F_TZ,
-  F_MU, F_T11, F_T22, F_T33, F_T12, F_T13, F_T23, F_HX, F_HY, F_HZ,
-  // divergence terms
-  F_M1, F_M2, F_M3,                         // mass: d1(ru) d2(rv) d3(rw)
-  F_A1X, F_A1Y, F_A1Z, F_PX, F_V1X, F_V1Y, F_V1Z,
-  F_A2X, F_A2Y, F_A2Z, F_PY, F_V2X, F_V2Y, F_V2Z,
-  F_A3X, F_A3Y, F_A3Z, F_PZ, F_V3X, F_V3Y, F_V3Z,
-  F_EX, F_EY, F_EZ, F_QX, F_QY, F_QZ,
-  kGenericFields
-};
 
 __global__ void k_prim(long long N, const double *__restrict__ q, double *__restrict__ t, double WoR) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
@@ -622,12 +451,12 @@ __global__ void k_assemble(long long N, const double *__restrict__ t, double *__
   }
 }
 
-void rhs_direct_generic(cruna_ctx *c, const double *q_in, double *rhs, double *qbc) {
+void rhs_direct_generic(cruna_ctx *c, const double *q_in, double *rhs, double *qbc, int bc_mask) {
   const long long N = c->g.N;
   double *t = c->tmp;
   auto F = [&](int f) { return t + (long long)f * N; };
   const double *q = q_in;
-  if (c->has_q_bc) {                                      // ns_rho_rhou_p.f90:89-92
+  if (c->has_q_bc && (bc_mask & 1)) {                     // ns_rho_rhou_p.f90:89-92
     copy_state(c, qbc, q_in, 5);
     bc_q(c, qbc, 0);
     q = qbc;
@@ -667,7 +496,28 @@ void rhs_direct_generic(cruna_ctx *c, const double *q_in, double *rhs, double *q
     apply_diff(c, d, F(F_HX + d), nullptr, F(F_QX + d), c->cfg.heat_flux_dx ? dx[d] : 1.0, 1);
   k_assemble<<<blocks, kThreads, 0, c->stream>>>(N, t, rhs, c->cfg.gamma, c->force);
   CRUNA_LAUNCH_CHECK(c);
-  if (c->has_rhs_bc) bc_rhs(c, rhs, q);                   // :218
+  if (c->has_rhs_bc && (bc_mask & 2)) bc_rhs(c, rhs, q);  // :218
+}
+
+// the forward part the discrete adjoint re-uses: u, T (:95-116), grad u, grad T, mu, tau, lambda grad T
+// (:102-128, :189-191) and grad p (:145, :159, :173) into the generic workspace
+void generic_forward_gradients(cruna_ctx *c, const double *q) {
+  const long long N = c->g.N;
+  double *t = c->tmp;
+  auto F = [&](int f) { return t + (long long)f * N; };
+  const int blocks = (int)std::min<long long>(nblocks(N), 148LL * 32);
+  k_prim<<<blocks, kThreads, 0, c->stream>>>(N, q, t, c->cfg.W / c->cfg.R);
+  CRUNA_LAUNCH_CHECK(c);
+  const double *dx = c->dx;
+  for (int v = 0; v < 3; ++v)
+    for (int d = 0; d < 3; ++d) apply_diff(c, d, F(F_U1 + v), nullptr, F(F_UX + 3 * v + d), dx[d], 1);
+  for (int d = 0; d < 3; ++d)
+    apply_diff(c, d, F(F_T), nullptr, F(F_TX + d), c->cfg.heat_flux_dx ? dx[d] : 1.0, 1);
+  k_visc<<<blocks, kThreads, 0, c->stream>>>(N, t, c->cfg.mu0, c->cfg.T0,
+                                             c->cfg.gamma * (c->cfg.R / c->cfg.W) / (c->cfg.gamma - 1.0) /
+                                                 c->cfg.Pr);
+  CRUNA_LAUNCH_CHECK(c);
+  for (int v = 0; v < 3; ++v) apply_diff(c, v, q + 4 * N, nullptr, F(F_PX + 7 * v), dx[v], 1);
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -68,6 +68,9 @@ void lapack_dgttrs(int n, const double *dl, const double *d, const double *du, c
 }
 
 static void factor(HostFactors &hf, int n) {
+  hf.raw_dl = hf.dl;
+  hf.raw_d = hf.d;
+  hf.raw_du = hf.du;
   hf.du2.assign(n > 2 ? n - 2 : 1, 0.0);
   hf.ipiv.assign(n, 0);
   hf.info = lapack_dgttrf(n, hf.dl.data(), hf.d.data(), hf.du.data(), hf.du2.data(), hf.ipiv.data());
