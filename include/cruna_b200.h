@@ -246,6 +246,31 @@ int cruna_step_direct_vjp(cruna_ctx *ctx, const double *q0, const double *lam1, 
 int cruna_step_direct_vjp_dev(cruna_ctx *ctx, const double *q0, const double *lam1, double *lam0,
                               double *grad_f, int nt);
 
+/* ---- learned subgrid closure (no counterpart in the reference: CRUNA has no learned component) ----
+   An MLP 12 -> 64 -> 64 -> 6 (GELU) from normalised features (the 9 velocity-gradient components
+   du_i/dx_j in the order (u_x, u_y, u_z, v_x, ..., w_z), density, temperature, filter width) to the 6
+   subgrid-stress components (tau_11, tau_22, tau_33, tau_12, tau_13, tau_23).  FP32 master parameters
+   (order W1[64][12], b1[64], W2[64][64], b2[64], W3[6][64], b3[6]); the kernels run BF16 operands with
+   FP32 accumulation on the tcgen05 tensor cores.  X is n x 12 and Y n x 6, row-major FP32 device
+   arrays; outputs are in physical units (network output times out_scale). */
+#define CRUNA_MLP_NPARAMS 5382
+typedef struct cruna_mlp cruna_mlp;
+int cruna_mlp_create(int device, uint64_t seed, cruna_mlp **out);
+void cruna_mlp_free(cruna_mlp *mlp);
+const char *cruna_mlp_last_error(const cruna_mlp *mlp);
+int cruna_mlp_set_params(cruna_mlp *mlp, const float *params);   /* host array, resets Adam state */
+int cruna_mlp_get_params(cruna_mlp *mlp, float *params);
+/* x_normalised = (x - in_mean) / in_scale; y = network output * out_scale */
+int cruna_mlp_set_scaling(cruna_mlp *mlp, const float *in_mean, const float *in_scale, const float *out_scale);
+int cruna_mlp_forward_dev(cruna_mlp *mlp, const float *X, float *Y, long long n);
+/* loss = mean over n x 6 of (y/out_scale - Y/out_scale)^2 and its gradient (host, 5382 floats);
+   n a multiple of 128 */
+int cruna_mlp_grad_dev(cruna_mlp *mlp, const float *X, const float *Y, int n, float *grad, float *loss);
+/* Adam (lr, beta 0.9 / 0.999, eps 1e-8) over `steps` mini-batches of `batch` samples (a multiple of
+   128) drawn without replacement per epoch (seeded shuffle); loss_hist (host, steps floats) may be NULL */
+int cruna_mlp_train_dev(cruna_mlp *mlp, const float *X, const float *Y, long long n, int batch, int steps,
+                        float lr, uint64_t seed, float *loss_hist);
+
 /* State check used by the run loops: returns CRUNA_ERR_STATE if any rho <= 0, p <= 0 or a
    non-finite value is found in q (device pointer). */
 int cruna_check_state_dev(cruna_ctx *ctx, const double *q);

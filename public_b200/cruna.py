@@ -115,6 +115,15 @@ _SIGNATURES = {
     "cruna_profile_enable": (_I, [_P, _I]),
     "cruna_profile_report": (_I, [_P, C.c_char_p, _I]),
     "cruna_rhs_direct_noalloc": (_I, [C.POINTER(_Config), _P, _P, _P, C.c_char_p, _I]),
+    "cruna_mlp_create": (_I, [_I, C.c_uint64, C.POINTER(_P)]),
+    "cruna_mlp_free": (None, [_P]),
+    "cruna_mlp_last_error": (C.c_char_p, [_P]),
+    "cruna_mlp_set_params": (_I, [_P, _P]),
+    "cruna_mlp_get_params": (_I, [_P, _P]),
+    "cruna_mlp_set_scaling": (_I, [_P, _P, _P, _P]),
+    "cruna_mlp_forward_dev": (_I, [_P, _P, _P, C.c_longlong]),
+    "cruna_mlp_grad_dev": (_I, [_P, _P, _P, _I, _P, C.POINTER(C.c_float)]),
+    "cruna_mlp_train_dev": (_I, [_P, _P, _P, C.c_longlong, _I, _I, C.c_float, C.c_uint64, _P]),
     "cruna_set_adjoint_mode": (_I, [_P, _I]),
     "cruna_rhs_direct_vjp": (_I, [_P, _P, _P, _P, _P]),
     "cruna_rhs_direct_vjp_dev": (_I, [_P, _P, _P, _P, _P]),
