@@ -271,6 +271,19 @@ int cruna_mlp_grad_dev(cruna_mlp *mlp, const float *X, const float *Y, int n, fl
 int cruna_mlp_train_dev(cruna_mlp *mlp, const float *X, const float *Y, long long n, int batch, int steps,
                         float lr, uint64_t seed, float *loss_hist);
 
+/* Box filter of a fine state by `factor` in every direction with more than one point (grid sizes
+   divisible by it): q_coarse (5 fields on the coarse grid) holds the means of rho, rho u_i and p; tau
+   (n_coarse x 6 floats, point-major, point order i fastest) the Favre subgrid stresses
+   mean(rho u_i u_j) - mean(rho u_i) mean(rho u_j) / mean(rho).  ctx is the fine grid's context. */
+int cruna_box_filter_dev(cruna_ctx *ctx, int factor, const double *q, double *q_coarse, float *tau);
+/* Closure features of a coarse state (n x 12 floats, point-major): du_i/dx_j with the context's
+   derivative scheme, rho, T, delta. */
+int cruna_closure_features_dev(cruna_ctx *ctx, const double *q, double delta, float *X);
+/* Attach (mlp != NULL) or detach the closure: every direct RHS evaluation of ctx then adds
+   -d_j tau_ij(model) to the momentum equations, on top of the forcing set with cruna_set_forcing.  The
+   MLP must outlive the attachment; the discrete adjoint (mode 1) is unavailable while attached. */
+int cruna_set_closure(cruna_ctx *ctx, cruna_mlp *mlp, double delta);
+
 /* State check used by the run loops: returns CRUNA_ERR_STATE if any rho <= 0, p <= 0 or a
    non-finite value is found in q (device pointer). */
 int cruna_check_state_dev(cruna_ctx *ctx, const double *q);

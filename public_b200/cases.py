@@ -176,6 +176,49 @@ def mixing_layer(n=(512, 384, 256), mach_c: float = 0.4, reynolds: float = 500.0
     return settings, q
 
 
+def isotropic_turbulence(n: int = 256, seed: int = 3, mach_t: float = 0.3, k0: float = 4.0,
+                         re_lambda: float = 100.0, cfl: float = 0.5) -> Tuple[Dict, np.ndarray]:
+    """Decaying isotropic turbulence in the periodic box [0, 2pi]^3: a solenoidal velocity field with
+    energy spectrum E(k) ~ k^4 exp(-2 (k/k0)^2) and random phases from PCG64(seed), scaled to the
+    turbulent Mach number sqrt(<u.u>)/c = mach_t; uniform rho = 1, p = 1/gamma (c = 1, R = W = 1, so
+    T = p / rho).  The viscosity gives Re_lambda = u' lambda / nu with u' = sqrt(<u.u>/3) and the
+    Taylor microscale lambda = sqrt(<u_x^2> / <(du_x/dx)^2>) of the initial field (spectral
+    derivatives); Sutherland's law is referenced to the initial temperature."""
+    g = GAMMA
+    L = 2.0 * math.pi
+    dx = L / n
+    rng = np.random.Generator(np.random.PCG64(seed))
+    k1 = np.fft.fftfreq(n, d=1.0 / n)
+    KX, KY, KZ = np.meshgrid(k1, k1, k1, indexing="ij")
+    K2 = KX ** 2 + KY ** 2 + KZ ** 2
+    Kmag = np.sqrt(K2)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        E = np.where(Kmag > 0, Kmag ** 4 * np.exp(-2.0 * (Kmag / k0) ** 2), 0.0)
+        amp = np.where(Kmag > 0, np.sqrt(E / (4.0 * math.pi * np.maximum(K2, 1e-30))), 0.0)
+    xi = [rng.standard_normal((n, n, n)) + 1j * rng.standard_normal((n, n, n)) for _ in range(3)]
+    kdx = (KX * xi[0] + KY * xi[1] + KZ * xi[2]) / np.where(K2 > 0, K2, 1.0)
+    uh = [amp * (xi[0] - KX * kdx), amp * (xi[1] - KY * kdx), amp * (xi[2] - KZ * kdx)]
+    u = [np.real(np.fft.ifftn(c)) for c in uh]
+    scale = mach_t / math.sqrt(float(np.mean(u[0] ** 2 + u[1] ** 2 + u[2] ** 2)))
+    u = [scale * c for c in u]
+    dudx = np.real(np.fft.ifftn(1j * KX * np.fft.fftn(u[0])))
+    lam = math.sqrt(float(np.mean(u[0] ** 2)) / float(np.mean(dudx ** 2)))
+    uprime = mach_t / math.sqrt(3.0)
+    nu = uprime * lam / re_lambda
+    rho0, p0 = 1.0, 1.0 / g
+    q = _state(n, n, n)
+    q[..., 0] = rho0
+    for v in range(3):
+        q[..., 1 + v] = rho0 * u[v]
+    q[..., 4] = p0
+    settings = dict(
+        n=(n, n, n), x0=(0.0, 0.0, 0.0), x1=(L, L, L),
+        diff=("o8_e_c_p",) * 3, filt=("o10_e_c_p",) * 3, alpha=0.0, strength=0.2,
+        di_freq=(1, 1, 1), gamma=g, R=1.0, W=1.0, mu0=rho0 * nu, T0=p0 / rho0, Pr=PR,
+        dt=_dt_cfl(q, dx, cfl, g))
+    return settings, q
+
+
 def smooth_random_state(n=(16, 12, 10), seed: int = 0, p0: float = 1.0, rho0: float = 1.0,
                         amp: float = 0.05, x1=(1.0, 1.0, 1.0)) -> np.ndarray:
     """A smooth positive state built from a few random Fourier modes (test input)."""

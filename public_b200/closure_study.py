@@ -1,0 +1,176 @@
+"""Learned subgrid closure study (the coarse-grid closure workload): decaying isotropic turbulence.
+
+1. Fine DNS on n^3 (8th-order differences, o10 filter every step, RK4) from
+   ``cases.isotropic_turbulence``; every ``every`` steps the solver box-filters the state by ``factor``
+   (``cruna_box_filter_dev``: filtered state and exact Favre subgrid stresses) and computes the
+   closure features on the coarse grid (``cruna_closure_features_dev``); a seeded random subset of the
+   coarse points of each snapshot becomes training pairs, and the filtered kinetic energy is recorded.
+2. The MLP (12 -> 64 -> 64 -> 6, BF16 tensor-core kernels) is trained with Adam on those pairs.
+3. Two coarse runs start from the filtered initial state with dt_c = (every / 2) dt_f: the plain
+   filter-stabilised coarse solve and the same solve with the closure attached (``cruna_set_closure``).
+   Their kinetic energy is compared with the filtered DNS at every snapshot time, and the GPU time of
+   each run (CUDA events, excluding set-up) with the fine DNS's.
+
+    python -m public_b200.closure_study [--n 256] [--factor 4] [--steps 3000] [--every 10]
+        [--samples 2000000] [--train-steps 3000] [--batch 4096] [--lr 1e-3] [--json out.json]
+
+Prints one JSON object.  Data are synthetic (seeded spectrum, no dataset).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+
+
+def kinetic_energy(q, dV: float) -> float:
+    """sum dV |rho u|^2 / (2 rho) of a Fortran-flattened device state (torch float64)."""
+    N = q.numel() // 5
+    rho, m = q[:N], q[N:4 * N].view(3, N)
+    return float(((m * m).sum(0) / (2.0 * rho)).sum().item()) * dV
+
+
+def run(args) -> dict:
+    import torch
+
+    from . import cases
+    from .closure import ClosureMLP
+    from .cruna import Cruna, Settings
+
+    dev = torch.device("cuda", 0)
+    s, q0 = cases.isotropic_turbulence(n=args.n, seed=args.seed, mach_t=args.mach_t, re_lambda=args.re_lambda)
+    nf, r = args.n, args.factor
+    nc = nf // r
+    dt_f = s["dt"]
+    if args.every % 2:
+        raise ValueError("--every must be even (coarse step = every/2 fine steps)")
+    dt_c = (args.every // 2) * dt_f
+    sc = dict(s, n=(nc, nc, nc), dt=dt_c)
+    L = s["x1"][0] - s["x0"][0]
+    dVf, dVc = (L / nf) ** 3, (L / nc) ** 3
+    delta = r * L / nf
+    Nc = nc ** 3
+    snaps = args.steps // args.every
+    per_snap = max(1, min(Nc, args.samples // max(snaps, 1)))
+    rng = torch.Generator(device=dev)
+    rng.manual_seed(args.seed + 17)
+
+    q = torch.from_numpy(np.ascontiguousarray(q0.ravel(order="F"))).to(dev)
+    qc = torch.empty(5 * Nc, dtype=torch.float64, device=dev)
+    tau = torch.empty((Nc, 6), dtype=torch.float32, device=dev)
+    feat = torch.empty((Nc, 12), dtype=torch.float32, device=dev)
+    Xs, Ys = [], []
+    ke_dns, t_dns = [], []
+    with Cruna(Settings.from_dict(s)) as fine, Cruna(Settings.from_dict(sc)) as coarse:
+        # initial filtered state (start of both coarse runs)
+        fine.box_filter_dev(r, q.data_ptr(), qc.data_ptr(), tau.data_ptr())
+        fine.sync()
+        qc0 = qc.clone()
+        ke_dns.append(kinetic_energy(qc, dVc))
+        t_dns.append(0.0)
+        dns_ms = 0.0
+        stream = torch.cuda.ExternalStream(fine.stream_handle(), device=dev)
+        for k in range(snaps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fine.run_direct_dev(q.data_ptr(), k * args.every, args.every)
+            e1.record(stream)
+            fine.box_filter_dev(r, q.data_ptr(), qc.data_ptr(), tau.data_ptr())
+            fine.sync()
+            dns_ms += e0.elapsed_time(e1)
+            coarse.closure_features_dev(qc.data_ptr(), delta, feat.data_ptr())
+            coarse.sync()
+            pick = torch.randperm(Nc, generator=rng, device=dev)[:per_snap]
+            Xs.append(feat[pick].clone())
+            Ys.append(tau[pick].clone())
+            ke_dns.append(kinetic_energy(qc, dVc))
+            t_dns.append((k + 1) * args.every * dt_f)
+        X = torch.cat(Xs).contiguous()
+        Y = torch.cat(Ys).contiguous()
+        in_mean = X.mean(0).cpu().numpy()
+        in_scale = X.std(0).cpu().numpy()
+        in_scale[in_scale <= 1e-12] = 1.0     # constant features (the filter width)
+        out_scale = Y.std(0).cpu().numpy()
+        out_scale[out_scale <= 1e-30] = 1.0
+        nb = (X.shape[0] // args.batch) * args.batch
+        X, Y = X[:nb].contiguous(), Y[:nb].contiguous()
+
+        mlp = ClosureMLP(0, seed=args.seed)
+        mlp.set_scaling(in_mean, in_scale, out_scale)
+        t0 = time.time()
+        hist = mlp.train(X, Y, batch=args.batch, steps=args.train_steps, lr=args.lr, seed=args.seed)
+        train_s = time.time() - t0
+        # explained variance of the stresses on the training pairs
+        pred = mlp.forward(X)
+        ev = 1.0 - float(((pred - Y) ** 2).sum().item()) / float(((Y - Y.mean(0)) ** 2).sum().item())
+
+        def coarse_run(with_closure: bool):
+            coarse.set_closure(mlp if with_closure else None, delta)
+            qq = qc0.clone()
+            ke, ms = [kinetic_energy(qq, dVc)], 0.0
+            cstream = torch.cuda.ExternalStream(coarse.stream_handle(), device=dev)
+            for k in range(snaps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(cstream)
+                coarse.run_direct_dev(qq.data_ptr(), k * 2, 2)
+                b.record(cstream)
+                coarse.sync()
+                ms += a.elapsed_time(b)
+                ke.append(kinetic_energy(qq, dVc))
+            coarse.set_closure(None)
+            return np.array(ke), ms
+
+        ke_plain, ms_plain = coarse_run(False)
+        ke_model, ms_model = coarse_run(True)
+        mlp.close()
+    ke_dns = np.array(ke_dns)
+
+    def err(ke):
+        return float(np.max(np.abs(ke - ke_dns) / ke_dns))
+
+    return {
+        "workload": f"isotropic turbulence {nf}^3 -> {nc}^3 (box filter x{r}), Mach_t {args.mach_t}, "
+                    f"Re_lambda {args.re_lambda}, {args.steps} fine steps",
+        "samples": int(X.shape[0]), "train_steps": args.train_steps, "batch": args.batch,
+        "train_loss_first": float(hist[0]) if len(hist) else None,
+        "train_loss_last": float(np.mean(hist[-20:])) if len(hist) else None,
+        "explained_variance": ev, "train_seconds": train_s,
+        "ke_decay_dns": float(ke_dns[-1] / ke_dns[0]),
+        "ke_max_rel_err_plain": err(ke_plain), "ke_max_rel_err_closure": err(ke_model),
+        "ke_final_rel_err_plain": float(abs(ke_plain[-1] - ke_dns[-1]) / ke_dns[-1]),
+        "ke_final_rel_err_closure": float(abs(ke_model[-1] - ke_dns[-1]) / ke_dns[-1]),
+        "gpu_ms_dns": dns_ms, "gpu_ms_coarse_plain": ms_plain, "gpu_ms_coarse_closure": ms_model,
+        "speedup_closure_vs_dns": dns_ms / ms_model if ms_model > 0 else None,
+        "times": [float(t) for t in t_dns], "ke_dns": ke_dns.tolist(), "ke_plain": ke_plain.tolist(),
+        "ke_closure": ke_model.tolist(),
+    }
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--factor", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--every", type=int, default=10)
+    ap.add_argument("--samples", type=int, default=2_000_000)
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--mach-t", type=float, default=0.3)
+    ap.add_argument("--re-lambda", type=float, default=100.0)
+    ap.add_argument("--json", type=str, default=None)
+    args = ap.parse_args(argv)
+    out = run(args)
+    line = json.dumps(out)
+    print(line)
+    if args.json:
+        with open(args.json, "w") as f:
+            f.write(line + "\n")
+
+
+if __name__ == "__main__":
+    main()

@@ -124,6 +124,9 @@ _SIGNATURES = {
     "cruna_mlp_forward_dev": (_I, [_P, _P, _P, C.c_longlong]),
     "cruna_mlp_grad_dev": (_I, [_P, _P, _P, _I, _P, C.POINTER(C.c_float)]),
     "cruna_mlp_train_dev": (_I, [_P, _P, _P, C.c_longlong, _I, _I, C.c_float, C.c_uint64, _P]),
+    "cruna_box_filter_dev": (_I, [_P, _I, _P, _P, _P]),
+    "cruna_closure_features_dev": (_I, [_P, _P, C.c_double, _P]),
+    "cruna_set_closure": (_I, [_P, _P, C.c_double]),
     "cruna_set_adjoint_mode": (_I, [_P, _I]),
     "cruna_rhs_direct_vjp": (_I, [_P, _P, _P, _P, _P]),
     "cruna_rhs_direct_vjp_dev": (_I, [_P, _P, _P, _P, _P]),
@@ -425,6 +428,20 @@ class Cruna:
         o.kind = {"plane_p2": 1, "kinetic_energy": 2}[kind]
         o.normal, o.index, o.p_inf = int(normal), int(index), float(p_inf)
         return o
+
+    # ---- learned closure (device pointers) ----
+    def box_filter_dev(self, factor: int, q_ptr: int, qc_ptr: int, tau_ptr: int):
+        """Box filter of the device state q into the coarse state and the subgrid stresses (floats)."""
+        self._check(self.lib.cruna_box_filter_dev(self.h, int(factor), C.c_void_p(q_ptr), C.c_void_p(qc_ptr),
+                                                  C.c_void_p(tau_ptr)))
+
+    def closure_features_dev(self, q_ptr: int, delta: float, x_ptr: int):
+        self._check(self.lib.cruna_closure_features_dev(self.h, C.c_void_p(q_ptr), float(delta), C.c_void_p(x_ptr)))
+
+    def set_closure(self, mlp, delta: float = 0.0):
+        """Attach a public_b200.closure.ClosureMLP (None detaches)."""
+        self._check(self.lib.cruna_set_closure(self.h, None if mlp is None else mlp.h, float(delta)))
+        self._closure = mlp  # keep the MLP alive while attached
 
     def set_adjoint_mode(self, mode: int):
         """0: the reference's continuous adjoint (default); 1: the exact discrete adjoint."""

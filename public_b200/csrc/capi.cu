@@ -118,19 +118,27 @@ void step_direct(cruna_ctx *c, const double *q0, double *q1) {
   double *k = c->st[0], *acc = c->st[1], *qa = c->st[2], *qb = c->st[3], *qbc = c->st[4];
   const double dt = c->cfg.dt;
   if (use_fused(c)) {
+    closure_stage(c, q0);
     rhs_direct_fused(c, q0, k, 1, q0, acc, qa, dt);
+    closure_stage(c, qa);
     rhs_direct_fused(c, qa, k, 2, q0, acc, qb, dt);
+    closure_stage(c, qb);
     rhs_direct_fused(c, qb, k, 3, q0, acc, qa, dt);
+    closure_stage(c, qa);
     rhs_direct_fused(c, qa, k, 4, q0, acc, q1, dt);
     return;
   }
   ensure_generic(c);
+  closure_stage(c, q0);
   rhs_direct_generic(c, q0, k, qbc);
   rk_stage(c, 1, dt, k, q0, acc, qa);
+  closure_stage(c, qa);
   rhs_direct_generic(c, qa, k, qbc);
   rk_stage(c, 2, dt, k, q0, acc, qb);
+  closure_stage(c, qb);
   rhs_direct_generic(c, qb, k, qbc);
   rk_stage(c, 3, dt, k, q0, acc, qa);
+  closure_stage(c, qa);
   rhs_direct_generic(c, qa, k, qbc);
   rk_stage(c, 4, dt, k, q0, acc, q1);
 }
@@ -507,15 +515,21 @@ int cruna_set_reference(cruna_ctx *c, const double *qref) {
   });
 }
 
+// the forcing the kernels add: the caller's, or (with a closure) the closure's buffer, which adds it
+void point_forcing(cruna_ctx *c, double *user) {
+  if (c->closure_mlp) c->user_force = user;
+  else c->force = user;
+}
+
 int cruna_set_forcing_dev(cruna_ctx *c, const double *f) {
   return guarded(c, [&]() -> int {
     if (!f) {
-      c->force = nullptr;
+      point_forcing(c, nullptr);
       return CRUNA_OK;
     }
     if (!c->io[3]) c->io[3] = dalloc(c, (size_t)N5(c));
     copy_state(c, c->io[3], f, 5);
-    c->force = c->io[3];
+    point_forcing(c, c->io[3]);
     return CRUNA_OK;
   });
 }
@@ -523,13 +537,13 @@ int cruna_set_forcing_dev(cruna_ctx *c, const double *f) {
 int cruna_set_forcing(cruna_ctx *c, const double *f) {
   return guarded(c, [&]() -> int {
     if (!f) {
-      c->force = nullptr;
+      point_forcing(c, nullptr);
       return CRUNA_OK;
     }
     if (!c->io[3]) c->io[3] = dalloc(c, (size_t)N5(c));
     CRUNA_CUDA_CHECK(cudaMemcpyAsync(c->io[3], f, sizeof(double) * N5(c), cudaMemcpyHostToDevice, c->stream));
     CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
-    c->force = c->io[3];
+    point_forcing(c, c->io[3]);
     return CRUNA_OK;
   });
 }
@@ -581,6 +595,7 @@ int cruna_filter(cruna_ctx *c, int dir, double *q, int nfields) {
 int cruna_rhs_direct_dev(cruna_ctx *c, const double *q, double *rhs, double /*t*/) {
   return guarded(c, [&]() -> int {
     if (!q || !rhs) fail(c, CRUNA_ERR_ARG, "null pointer");
+    closure_stage(c, q);
     if (use_fused(c)) {
       rhs_direct_fused(c, q, rhs, 0, nullptr, nullptr, nullptr, 0.0);
     } else {
@@ -907,6 +922,8 @@ int cruna_set_adjoint_mode(cruna_ctx *c, int mode) {
     if (mode != 0 && mode != 1) fail(c, CRUNA_ERR_ARG, "adjoint mode must be 0 (continuous) or 1 (discrete)");
     if (mode == 1 && c->cfg.precision != CRUNA_FP64)
       fail(c, CRUNA_ERR_UNSUPPORTED, "the discrete adjoint needs precision CRUNA_FP64");
+    if (mode == 1 && c->closure_mlp)
+      fail(c, CRUNA_ERR_UNSUPPORTED, "the discrete adjoint does not transpose the closure");
     c->adjoint_mode = mode;
     return CRUNA_OK;
   });

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/cruna_b200.h"
+#include "cruna_internal.cuh"
 #include "tcgen05.cuh"
 
 namespace cruna {
@@ -583,6 +584,24 @@ void run_grad(cruna_mlp *h, const float *X, const float *Y, const int *idx, int 
 }
 
 }  // namespace
+
+namespace cruna {
+// forward pass enqueued on a caller's stream (the coarse solver's), no host synchronisation; a wait that
+// timed out inside the kernel raises the MLP's error flag, reported by its next checked call
+void mlp_forward_stream(cruna_mlp *h, const float *X, float *Y, long long n, cudaStream_t stream) {
+  try {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    if (n <= 0) return;
+    set_attrs(h);
+    const long long tiles = (n + 127) / 128;
+    const int nblk = (int)std::min<long long>(tiles, 4LL * sm_count(h->device));
+    k_mlp_forward<<<nblk, 128, sizeof(FwdSmem), stream>>>(h->P, h->sc, X, Y, n, h->flag);
+    ck(cudaGetLastError(), "k_mlp_forward launch");
+  } catch (const MlpError &e) {
+    throw ApiError{e.code, e.msg};
+  }
+}
+}  // namespace cruna
 
 extern "C" {
 

@@ -152,6 +152,13 @@ struct cruna_ctx {
   std::vector<double *> vjp_save;  // per boundary row: box values before the row (q, aim / rhs)
   double *vjp_gf = nullptr;        // staging of grad_f for the host-pointer entry points (io[3] holds f)
   int adjoint_mode = 0;            // cruna_gradient: 0 continuous (reference), 1 discrete
+  // learned subgrid closure (closure_ops.cu): active when mlp is set
+  struct cruna_mlp *closure_mlp = nullptr;
+  double closure_delta = 0.0;
+  double *user_force = nullptr;    // the caller's forcing (cruna_set_forcing) while a closure is set
+  double *cl_force = nullptr;      // forcing + closure stress divergence (5N)
+  double *cl_tau = nullptr;        // model stresses (6N) and their derivatives (9N)
+  float *cl_x = nullptr, *cl_y = nullptr;  // features (12N) and outputs (6N), point-major
 };
 
 namespace cruna {
@@ -188,6 +195,9 @@ int check_state(cruna_ctx *c, const double *q);
 double *dalloc(cruna_ctx *c, size_t count);
 void ensure_generic(cruna_ctx *c);
 bool use_fused(const cruna_ctx *c);
+// learned closure (closure_mlp.cu, closure_ops.cu)
+void mlp_forward_stream(struct cruna_mlp *h, const float *X, float *Y, long long n, cudaStream_t stream);
+void closure_stage(cruna_ctx *c, const double *q);  // sets c->force for the next direct RHS evaluation
 // discrete adjoint (discrete_adjoint.cu)
 void rhs_direct_vjp(cruna_ctx *c, const double *q, const double *lam, double *mu, double *gf_acc);
 void step_direct_vjp(cruna_ctx *c, const double *q0, const double *lam1, double *lam0, double *gf_acc,

@@ -1,0 +1,117 @@
+"""GPU tests of the closure plumbing around the solver: box filter and exact subgrid stresses, closure
+features, the closure term inside the coarse RHS, and a small end-to-end closure study."""
+import numpy as np
+import pytest
+
+from oracle import cruna_oracle as O
+from oracle import mlp_closure as M
+from public_b200 import cases
+from public_b200.cruna import Cruna, Settings
+
+pytestmark = pytest.mark.gpu
+
+CFG_FIELDS = {f.name for f in O.dataclasses.fields(O.Config)}
+
+
+def ocfg(s):
+    return O.Config(**{k: v for k, v in s.items() if k in CFG_FIELDS})
+
+
+def dev(a, dtype=None):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    return t.cuda() if dtype is None else t.to(dtype).cuda()
+
+
+def flat(q):
+    return np.ascontiguousarray(q.ravel(order="F"))
+
+
+def test_box_filter_and_subgrid_stress():
+    import torch
+    s, q = cases.isotropic_turbulence(n=16, seed=1)
+    r, nc = 4, 4
+    qd = dev(flat(q))
+    qc = torch.empty(5 * nc ** 3, dtype=torch.float64, device="cuda")
+    tau = torch.empty((nc ** 3, 6), dtype=torch.float32, device="cuda")
+    with Cruna(Settings.from_dict(s)) as c:
+        c.box_filter_dev(r, qd.data_ptr(), qc.data_ptr(), tau.data_ptr())
+        c.sync()
+    blk = lambda f: f.reshape(nc, r, nc, r, nc, r).mean(axis=(1, 3, 5))
+    rho = q[..., 0]
+    ref_q = np.stack([blk(q[..., v]) for v in range(5)], axis=-1)
+    got_q = qc.cpu().numpy().reshape((nc, nc, nc, 5), order="F")
+    assert np.max(np.abs(got_q - ref_q)) < 1e-14 * np.max(np.abs(ref_q))
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    got_t = tau.cpu().numpy()
+    for t, (i, j) in enumerate(pairs):
+        ref = blk(q[..., 1 + i] * q[..., 1 + j] / rho) - ref_q[..., 1 + i] * ref_q[..., 1 + j] / ref_q[..., 0]
+        got = got_t[:, t].reshape((nc, nc, nc), order="F")
+        assert np.max(np.abs(got - ref)) < 1e-6 * np.max(np.abs(ref)) + 1e-12, (i, j)
+
+
+def test_closure_features_match_oracle():
+    import torch
+    s, q = cases.isotropic_turbulence(n=16, seed=2)
+    cfg = ocfg(s)
+    dx = cfg.dx()
+    X = torch.empty((16 ** 3, 12), dtype=torch.float32, device="cuda")
+    with Cruna(Settings.from_dict(s)) as c:
+        c.closure_features_dev(dev(flat(q)).data_ptr(), 0.5, X.data_ptr())
+        c.sync()
+    got = X.cpu().numpy()
+    u = [q[..., 1 + v] / q[..., 0] for v in range(3)]
+    ref = [O.Dx(cfg, d, u[v], dx[d]) for v in range(3) for d in range(3)]
+    ref += [q[..., 0], O.give_T(cfg, q), np.full(q.shape[:3], 0.5)]
+    for k, r in enumerate(ref):
+        g = got[:, k].reshape(q.shape[:3], order="F")
+        assert np.max(np.abs(g - r)) <= 1e-6 * np.max(np.abs(r)) + 1e-7, k
+
+
+def test_closure_adds_model_stress_divergence():
+    """rhs(closure) - rhs(plain) = -d_j tau_ij(model) in the momentum equations, 0 elsewhere."""
+    import torch
+
+    from public_b200.closure import ClosureMLP
+    s, q = cases.isotropic_turbulence(n=16, seed=3)
+    cfg = ocfg(s)
+    dx = cfg.dx()
+    f = cases.smooth_random_state((16, 16, 16), seed=2, p0=0.0, rho0=0.0, amp=0.01)
+    with Cruna(Settings.from_dict(s), force=f) as c, ClosureMLP(0, seed=4) as mlp:
+        mlp.params = M.init_params(7)
+        mlp.set_scaling(np.zeros(12), np.ones(12), np.full(6, 1e-3))
+        X = torch.empty((16 ** 3, 12), dtype=torch.float32, device="cuda")
+        c.closure_features_dev(dev(flat(q)).data_ptr(), 0.3, X.data_ptr())
+        c.sync()
+        tau = mlp.forward(X).cpu().numpy().astype(np.float64)
+        plain = c.rhs_direct(q)
+        c.set_closure(mlp, 0.3)
+        with_cl = c.rhs_direct(q)
+        c.set_forcing(None)        # forcing removed while the closure stays attached
+        no_f = c.rhs_direct(q)
+        c.set_closure(None)
+        back = c.rhs_direct(q)
+    T = [tau[:, t].reshape(q.shape[:3], order="F") for t in range(6)]
+    idx = {(0, 0): 0, (1, 1): 1, (2, 2): 2, (0, 1): 3, (1, 0): 3, (0, 2): 4, (2, 0): 4, (1, 2): 5, (2, 1): 5}
+    diff = with_cl - plain
+    for i in range(3):
+        div = sum(O.Dx(cfg, j, T[idx[(i, j)]], dx[j]) for j in range(3))
+        assert np.max(np.abs(diff[..., 1 + i] + div)) < 1e-9 * np.max(np.abs(div)) + 1e-12, i
+    assert np.max(np.abs(diff[..., 0])) < 1e-12 and np.max(np.abs(diff[..., 4])) < 1e-12 * np.max(np.abs(plain))
+    assert np.max(np.abs((with_cl - no_f) - f)) < 1e-12 * max(1.0, np.max(np.abs(f)))
+    assert np.max(np.abs(back - no_f + (with_cl - plain))) < 1e-9 * np.max(np.abs(plain))
+
+
+def test_small_closure_study_runs_end_to_end():
+    from public_b200 import closure_study
+    import argparse
+    args = argparse.Namespace(
+        n=64, factor=4, steps=40, every=10, samples=8192, train_steps=60, batch=512, lr=2e-3, seed=3,
+        mach_t=0.3, re_lambda=60.0, json=None)
+    out = closure_study.run(args)
+    assert out["samples"] >= 512
+    assert out["train_loss_last"] < out["train_loss_first"]
+    for key in ("ke_dns", "ke_plain", "ke_closure"):
+        assert len(out[key]) == 5 and all(np.isfinite(out[key]))
+    assert out["ke_decay_dns"] < 1.0
+    assert out["ke_max_rel_err_plain"] < 0.2 and out["ke_max_rel_err_closure"] < 0.2
