@@ -223,6 +223,18 @@ int cruna_gradient(cruna_ctx *ctx, const double *q0, int nsteps, int nsnap, cons
 int cruna_gradient_dev(cruna_ctx *ctx, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
                        double *J, double *grad_f, double *grad_q0, int64_t *direct_steps);
 
+/* z-slab decomposition (replaces the reference's MPI pencil transposes, transpose_mpi_cartesian.f90,
+   for runs over several GPUs): the context holds one slab of the global grid extended by H >= 2R halo
+   planes on each side (n3 = nz_local + 2H, periodic z scheme of half-width R), and before every pass
+   that reads z-neighbours (each RK stage of the direct and adjoint steps, the frozen direct state of
+   an adjoint step, the z filter) the library calls fn(user, fields, nfields, stream): it must refresh
+   the H lowest and H highest planes of each of the nfields fields (device pointer, Fortran layout)
+   with the neighbouring slabs' interior planes, ordered on `stream` (a cudaStream_t).  Interior results
+   are then exactly the single-domain ones; halo planes hold no meaningful values between calls.
+   fn returns 0 on success.  NULL detaches. */
+int cruna_set_halo_exchange(cruna_ctx *ctx, int (*fn)(void *user, double *fields, int nfields, void *stream),
+                            void *user);
+
 /* Adjoint used by cruna_gradient: 0 = the reference's continuous inviscid adjoint step
    (right_hand_side_adjoint_3d, ns_rho_rhou_p.f90:257-536, integrated by time_stepper_adjoint,
    rk_o4_e.f90:62-105; the default), 1 = the exact discrete adjoint (no counterpart in the reference):

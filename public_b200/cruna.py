@@ -127,6 +127,7 @@ _SIGNATURES = {
     "cruna_box_filter_dev": (_I, [_P, _I, _P, _P, _P]),
     "cruna_closure_features_dev": (_I, [_P, _P, C.c_double, _P]),
     "cruna_set_closure": (_I, [_P, _P, C.c_double]),
+    "cruna_set_halo_exchange": (_I, [_P, _P, _P]),
     "cruna_set_adjoint_mode": (_I, [_P, _I]),
     "cruna_rhs_direct_vjp": (_I, [_P, _P, _P, _P, _P]),
     "cruna_rhs_direct_vjp_dev": (_I, [_P, _P, _P, _P, _P]),
@@ -442,6 +443,11 @@ class Cruna:
         """Attach a public_b200.closure.ClosureMLP (None detaches)."""
         self._check(self.lib.cruna_set_closure(self.h, None if mlp is None else mlp.h, float(delta)))
         self._closure = mlp  # keep the MLP alive while attached
+
+    def set_halo_exchange(self, fn):
+        """Install a z-slab halo callback (a ctypes function of public_b200.slabs.HALO_FN; None detaches)."""
+        self._check(self.lib.cruna_set_halo_exchange(self.h, None if fn is None else C.cast(fn, C.c_void_p), None))
+        self._halo_fn = fn
 
     def set_adjoint_mode(self, mode: int):
         """0: the reference's continuous adjoint (default); 1: the exact discrete adjoint."""

@@ -29,6 +29,13 @@ void ensure_generic(cruna_ctx *c) {
 
 bool use_fused(const cruna_ctx *c) { return c->fused_ok && !c->force_generic; }
 
+// z-slab mode: let the caller refresh the halo planes of `nfields` fields before a z-reading pass
+void halo(cruna_ctx *c, const double *f, int nfields) {
+  if (!c->halo_fn) return;
+  if (c->halo_fn(c->halo_user, const_cast<double *>(f), nfields, (void *)c->stream) != 0)
+    throw ApiError{CRUNA_ERR_CUDA, "halo exchange callback failed"};
+}
+
 }  // namespace cruna
 
 namespace {
@@ -118,26 +125,34 @@ void step_direct(cruna_ctx *c, const double *q0, double *q1) {
   double *k = c->st[0], *acc = c->st[1], *qa = c->st[2], *qb = c->st[3], *qbc = c->st[4];
   const double dt = c->cfg.dt;
   if (use_fused(c)) {
+    halo(c, q0, 5);
     closure_stage(c, q0);
     rhs_direct_fused(c, q0, k, 1, q0, acc, qa, dt);
+    halo(c, qa, 5);
     closure_stage(c, qa);
     rhs_direct_fused(c, qa, k, 2, q0, acc, qb, dt);
+    halo(c, qb, 5);
     closure_stage(c, qb);
     rhs_direct_fused(c, qb, k, 3, q0, acc, qa, dt);
+    halo(c, qa, 5);
     closure_stage(c, qa);
     rhs_direct_fused(c, qa, k, 4, q0, acc, q1, dt);
     return;
   }
   ensure_generic(c);
+  halo(c, q0, 5);
   closure_stage(c, q0);
   rhs_direct_generic(c, q0, k, qbc);
   rk_stage(c, 1, dt, k, q0, acc, qa);
+  halo(c, qa, 5);
   closure_stage(c, qa);
   rhs_direct_generic(c, qa, k, qbc);
   rk_stage(c, 2, dt, k, q0, acc, qb);
+  halo(c, qb, 5);
   closure_stage(c, qb);
   rhs_direct_generic(c, qb, k, qbc);
   rk_stage(c, 3, dt, k, q0, acc, qa);
+  halo(c, qa, 5);
   closure_stage(c, qa);
   rhs_direct_generic(c, qa, k, qbc);
   rk_stage(c, 4, dt, k, q0, acc, q1);
@@ -147,20 +162,29 @@ void step_direct(cruna_ctx *c, const double *q0, double *q1) {
 void step_adjoint(cruna_ctx *c, const double *qs0, const double *q0, const double *g, double *qs1) {
   double *k = c->st[0], *acc = c->st[1], *qa = c->st[2], *qb = c->st[3], *qbc = c->st[4];
   const double dt = -c->cfg.dt;
+  halo(c, q0, 5);
   if (use_fused(c)) {
+    halo(c, qs0, 5);
     rhs_adjoint_fused(c, qs0, q0, g, k, 1, qs0, acc, qa, dt);
+    halo(c, qa, 5);
     rhs_adjoint_fused(c, qa, q0, g, k, 2, qs0, acc, qb, dt);
+    halo(c, qb, 5);
     rhs_adjoint_fused(c, qb, q0, g, k, 3, qs0, acc, qa, dt);
+    halo(c, qa, 5);
     rhs_adjoint_fused(c, qa, q0, g, k, 4, qs0, acc, qs1, dt);
     return;
   }
   ensure_generic(c);
+  halo(c, qs0, 5);
   rhs_adjoint_generic(c, qs0, q0, g, k, qbc);
   rk_stage(c, 1, dt, k, qs0, acc, qa);
+  halo(c, qa, 5);
   rhs_adjoint_generic(c, qa, q0, g, k, qbc);
   rk_stage(c, 2, dt, k, qs0, acc, qb);
+  halo(c, qb, 5);
   rhs_adjoint_generic(c, qb, q0, g, k, qbc);
   rk_stage(c, 3, dt, k, qs0, acc, qa);
+  halo(c, qa, 5);
   rhs_adjoint_generic(c, qa, q0, g, k, qbc);
   rk_stage(c, 4, dt, k, qs0, acc, qs1);
 }
@@ -778,10 +802,12 @@ void direct_loop_step(cruna_ctx *c, double *q, int nt) {
   if (c->filter_fused_ok && !c->force_generic && (on[0] || on[1] || on[2])) {
     step_direct(c, q, c->st[5]);
     if (c->has_q_bc) bc_q(c, c->st[5], 1);
+    if (on[2]) halo(c, c->st[5], 5);
     filter3_fused(c, c->st[5], q, on);
   } else {
     step_direct(c, q, q);
     if (c->has_q_bc) bc_q(c, q, 1);
+    if (on[2]) halo(c, q, 5);
     for (int d = 0; d < 3; ++d)
       if (on[d]) apply_filter(c, d, q, c->st[5], 5);
   }
@@ -794,10 +820,12 @@ void adjoint_loop_step(cruna_ctx *c, double *qs, const double *q0, const double 
   if (c->filter_fused_ok && !c->force_generic && (on[0] || on[1] || on[2])) {
     step_adjoint(c, qs, q0, g, c->st[5]);
     if (c->has_q_bc) bc_qs(c, c->st[5], q0, 1);
+    if (on[2]) halo(c, c->st[5], 5);
     filter3_fused(c, c->st[5], qs, on);
   } else {
     step_adjoint(c, qs, q0, g, qs);
     if (c->has_q_bc) bc_qs(c, qs, q0, 1);
+    if (on[2]) halo(c, qs, 5);
     for (int d = 0; d < 3; ++d)
       if (on[d]) apply_filter(c, d, qs, c->st[5], 5);
   }
@@ -889,6 +917,7 @@ int cruna_run_adjoint(cruna_ctx *c, double *qs_io, const double *Q_traj, const d
 static int gradient_common(cruna_ctx *c, const double *q0_dev, int nsteps, int nsnap, const cruna_objective *obj,
                            double *J, double *gf_dev, double *gq_dev, int64_t *direct_steps) {
   if (!q0_dev || !obj || !J || nsteps < 1 || nsnap < 1) fail(c, CRUNA_ERR_ARG, "bad arguments to cruna_gradient");
+  if (c->halo_fn) fail(c, CRUNA_ERR_UNSUPPORTED, "objective reductions over z slabs are not provided");
   if (obj->kind != CRUNA_OBJ_PLANE_P2 && obj->kind != CRUNA_OBJ_KINETIC_ENERGY)
     fail(c, CRUNA_ERR_ARG, "unknown objective kind");
   if (obj->kind == CRUNA_OBJ_PLANE_P2) {
@@ -915,6 +944,16 @@ static int gradient_common(cruna_ctx *c, const double *q0_dev, int nsteps, int n
   for (void *q : scratch) cudaFree(q);
   if (direct_steps) *direct_steps = adv;
   return CRUNA_OK;
+}
+
+int cruna_set_halo_exchange(cruna_ctx *c, int (*fn)(void *, double *, int, void *), void *user) {
+  return guarded(c, [&]() -> int {
+    if (fn && (c->dop[2].kind != OP_STENCIL || !c->dop[2].periodic || c->has_q_bc || c->has_rhs_bc))
+      fail(c, CRUNA_ERR_UNSUPPORTED, "z slabs need a periodic z scheme and no boundary table");
+    c->halo_fn = fn;
+    c->halo_user = user;
+    return CRUNA_OK;
+  });
 }
 
 int cruna_set_adjoint_mode(cruna_ctx *c, int mode) {

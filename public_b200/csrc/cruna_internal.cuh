@@ -152,6 +152,9 @@ struct cruna_ctx {
   std::vector<double *> vjp_save;  // per boundary row: box values before the row (q, aim / rhs)
   double *vjp_gf = nullptr;        // staging of grad_f for the host-pointer entry points (io[3] holds f)
   int adjoint_mode = 0;            // cruna_gradient: 0 continuous (reference), 1 discrete
+  // z-slab decomposition: refreshes the halo planes of a state before a pass that reads z-neighbours
+  int (*halo_fn)(void *user, double *fields, int nfields, void *stream) = nullptr;
+  void *halo_user = nullptr;
   // learned subgrid closure (closure_ops.cu): active when mlp is set
   struct cruna_mlp *closure_mlp = nullptr;
   double closure_delta = 0.0;

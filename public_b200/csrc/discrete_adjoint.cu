@@ -552,6 +552,7 @@ void ensure_vjp(cruna_ctx *c) {
   if (c->cfg.precision != CRUNA_FP64)
     throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint transposes the FP64 operator: precision must be FP64"};
   if (c->closure_mlp) throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint does not transpose the closure"};
+  if (c->halo_fn) throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint runs on one block (no z slabs)"};
   for (int d = 0; d < 3; ++d) {
     build_transpose(c, c->dop[d], c->dhf[d], c->dopT[d]);
     build_transpose(c, c->fop[d], c->fhf[d], c->fopT[d]);
