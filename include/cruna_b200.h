@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define CRUNA_ABI_VERSION 1
+#define CRUNA_ABI_VERSION 2
 
 /* status codes */
 #define CRUNA_OK 0
@@ -96,6 +96,9 @@ typedef struct cruna_config {
   int32_t sponge_shape;          /* sponge.shape: 0 quadratic, 1 cos */
   int32_t device;                /* CUDA device ordinal */
   int32_t check_every;           /* >0: run-loops check rho>0, p>0, finiteness every N steps */
+  int32_t kvector;               /* sponge.kvector for the zonal BC types 202/203/205/206
+                                    (boundary_conditions.f90:414-420): 0 diagonal, 1 orthogonal,
+                                    2 hedgehog (boundary_normal_vector.f90:37-261) */
 } cruna_config;
 
 typedef struct cruna_ctx cruna_ctx;

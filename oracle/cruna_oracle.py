@@ -424,6 +424,7 @@ class Config:
     sponge_length: Tuple[float, float, float] = (0.3, 0.3, 0.3)
     sponge_amplitude: float = 1.0
     sponge_shape: str = "quadratic"
+    kvector: str = "diagonal"         # sponge.kvector: diagonal, orthogonal, hedgehog (zonal BC types)
 
     @property
     def npts(self) -> int:
@@ -549,8 +550,36 @@ def _box(row) -> Tuple[slice, slice, slice]:
     return slice(is_ - 1, ie), slice(js - 1, je), slice(ks - 1, ke)
 
 
-def characteristic_q_k1d(cfg: Config, q: np.ndarray, aim: np.ndarray, kvec) -> np.ndarray:
-    """nonreflecting.f90:46-137 on a box (q, aim have shape (..., 5)); returns the new q."""
+def kvector_field(cfg: Config) -> np.ndarray:
+    """Boundary normal vectors (n1, n2, n3, 3) of the zonal BC types: init_orthogonal_and_diagonal_kvector,
+    init_orthogonal_kvector, init_hedgehog_kvector and normalize_kvector (boundary_normal_vector.f90:37-261)."""
+    x = cfg.grid()
+    L = [cfg.x1[d] - cfg.x0[d] for d in range(3)]
+    X = np.meshgrid(*x, indexing="ij")
+    k = np.stack([X[d] - (cfg.x0[d] + 0.5 * L[d]) for d in range(3)], axis=-1)
+    if cfg.kvector == "hedgehog":
+        return k / np.sqrt(np.sum(k ** 2, axis=-1))[..., None]
+    k = k / np.array(L)
+    dx = cfg.dx()
+    half = 0.5 * min(dx[d] / L[d] for d in range(3))
+    a = np.abs(k)
+    m = a.max(axis=-1)
+    dom = np.where(m == a[..., 0], 0, np.where(m == a[..., 1], 1, 2))
+    out = np.zeros_like(k)
+    for d in range(3):
+        sgn = np.copysign(1.0, k[..., d])
+        keep = (dom == d)
+        if cfg.kvector == "diagonal":
+            keep = keep | (m - a[..., d] < half)
+        out[..., d] = np.where(keep, sgn, 0.0)
+    if cfg.kvector == "diagonal":
+        out = out / np.sqrt(np.sum(out ** 2, axis=-1))[..., None]
+    return out
+
+
+def characteristic_q_k1d(cfg: Config, q: np.ndarray, aim: np.ndarray, kvec, shape=None) -> np.ndarray:
+    """nonreflecting.f90:46-137 on a box (q, aim have shape (..., 5)); returns the new q.  With kvec of
+    shape (..., 3) and an optional shape factor this is characteristic_q_k4d (:141-233)."""
     r = q[..., 0]
     u = q[..., 1:4] / r[..., None]
     p = q[..., 4]
@@ -559,7 +588,10 @@ def characteristic_q_k1d(cfg: Config, q: np.ndarray, aim: np.ndarray, kvec) -> n
     dq[..., 0] = aim[..., 0] - r
     dq[..., 1:4] = aim[..., 1:4] / aim[..., 0:1] - u
     dq[..., 4] = aim[..., 4] - p
-    kx, ky, kz = -kvec[0], -kvec[1], -kvec[2]
+    if shape is not None:
+        dq = dq * shape[..., None]
+    kvec = np.asarray(kvec)
+    kx, ky, kz = -kvec[..., 0], -kvec[..., 1], -kvec[..., 2]
     c2 = c ** 2
     R1 = kx * dq[..., 0] + kz * dq[..., 2] - ky * dq[..., 3] - kx * dq[..., 4] / c2
     R2 = ky * dq[..., 0] - kz * dq[..., 1] + kx * dq[..., 3] - ky * dq[..., 4] / c2
@@ -593,8 +625,9 @@ def characteristic_q_k1d(cfg: Config, q: np.ndarray, aim: np.ndarray, kvec) -> n
     return out
 
 
-def characteristic_rhs_k1d(cfg: Config, rhs, q, aim, kvec) -> np.ndarray:
-    """nonreflecting.f90:237-341 without shape (BC type 204)."""
+def characteristic_rhs_k1d(cfg: Config, rhs, q, aim, kvec, shape=None) -> np.ndarray:
+    """nonreflecting.f90:237-341 without shape (BC type 204); with kvec (..., 3) and shape it is
+    characteristic_rhs_k4d (:345-449, types 205 and 206)."""
     dt = cfg.dt
     inv_dt = 1.0 / dt
     r = q[..., 0]
@@ -610,7 +643,8 @@ def characteristic_rhs_k1d(cfg: Config, rhs, q, aim, kvec) -> np.ndarray:
     dq[..., 2] = dq[..., 2] + rhs[..., 2] * tmp
     dq[..., 3] = dq[..., 3] + rhs[..., 3] * tmp
     dq[..., 4] = dq[..., 4] + rhs[..., 4] * dt
-    kx, ky, kz = -kvec[0], -kvec[1], -kvec[2]
+    kvec = np.asarray(kvec)
+    kx, ky, kz = -kvec[..., 0], -kvec[..., 1], -kvec[..., 2]
     c2 = c ** 2
     R1 = kx * dq[..., 0] + kz * dq[..., 2] - ky * dq[..., 3] - kx * dq[..., 4] / c2
     R2 = ky * dq[..., 0] - kz * dq[..., 1] + kx * dq[..., 3] - ky * dq[..., 4] / c2
@@ -632,6 +666,15 @@ def characteristic_rhs_k1d(cfg: Config, rhs, q, aim, kvec) -> np.ndarray:
     d5 = +0.5 * r * c * R4 + 0.5 * r * c * R5
     r = r + d1
     out = np.empty_like(rhs)
+    if shape is not None:                                       # :428-435
+        tmp = shape * inv_dt
+        out[..., 0] = (1.0 - shape) * rhs[..., 0] + d1 * tmp
+        out[..., 4] = (1.0 - shape) * rhs[..., 4] + d5 * tmp
+        tmp = tmp * r
+        out[..., 1] = (1.0 - shape) * rhs[..., 1] + d2 * tmp
+        out[..., 2] = (1.0 - shape) * rhs[..., 2] + d3 * tmp
+        out[..., 3] = (1.0 - shape) * rhs[..., 3] + d4 * tmp
+        return out
     out[..., 0] = d1 * inv_dt
     tmp = inv_dt * r
     out[..., 1] = d2 * tmp
@@ -641,10 +684,14 @@ def characteristic_rhs_k1d(cfg: Config, rhs, q, aim, kvec) -> np.ndarray:
     return out
 
 
-def characteristic_qs_k1d(cfg: Config, qs, q, kvec) -> np.ndarray:
-    """nonreflecting.f90:453-554 (adjoint, target zero)."""
+def characteristic_qs_k1d(cfg: Config, qs, q, kvec, shape=None) -> np.ndarray:
+    """nonreflecting.f90:453-554 (adjoint, target zero); with kvec (..., 3) and shape it is
+    characteristic_qs_k4d (:558-661)."""
     ds = -qs
-    kx, ky, kz = -kvec[0], -kvec[1], -kvec[2]
+    if shape is not None:
+        ds = ds * shape[..., None]
+    kvec = np.asarray(kvec)
+    kx, ky, kz = -kvec[..., 0], -kvec[..., 1], -kvec[..., 2]
     gm1 = cfg.gamma - 1.0
     c = np.sqrt(cfg.gamma * (q[..., 4] / q[..., 0]))
     g_c = gm1 / c
@@ -685,6 +732,13 @@ def characteristic_qs_k1d(cfg: Config, qs, q, kvec) -> np.ndarray:
     return out
 
 
+def _zonal_active(row, outside_rhs: bool) -> bool:
+    """Type 203 inside / outside the RHS: column 8 = -1 applies outside only, 1 inside only
+    (boundary_conditions.f90:96-107, :436-438)."""
+    only = int(round(row[7]))
+    return (only != 1) if outside_rhs else (only != -1)
+
+
 def _zero_grad_shift(row) -> Tuple[int, int, int]:
     """characteristic_zero_grad_init (nonreflecting.f90:665-700): unit step towards the inside."""
     k = np.array(row[7:10], dtype=np.float64)
@@ -702,11 +756,13 @@ class Solver:
         self.qref = qref
         self.force = force
         self.bc = np.zeros((0, 10)) if cfg.bc is None else np.asarray(cfg.bc, dtype=np.float64)
-        need_shape = any(int(round(r[0])) in (400, 401) for r in self.bc)
+        need_shape = any(int(round(r[0])) in (203, 206, 400, 401) for r in self.bc)
         self.shape = sponge_shape(cfg) if need_shape else None
+        zonal = any(int(round(r[0])) in (202, 203, 205, 206) for r in self.bc)
+        self.kvec = kvector_field(cfg) if zonal else None
         for r in self.bc:
             t = int(round(r[0]))
-            if t not in (0, 100, 200, 201, 204, 400, 401):
+            if t not in (0, 100, 200, 201, 202, 203, 204, 205, 206, 400, 401):
                 raise NotImplementedError(f"boundary type {t} is not on this path")
 
     # --------------------------------------------------------------------------------------------
@@ -722,6 +778,10 @@ class Solver:
                 q[b] = characteristic_q_k1d(self.cfg, q[b], q[b2], row[7:10])
             elif t == 201:
                 q[b] = characteristic_q_k1d(self.cfg, q[b], self.qref[b], row[7:10])
+            elif t == 202:                                          # boundary_conditions.f90:89-91
+                q[b] = characteristic_q_k1d(self.cfg, q[b], self.qref[b], self.kvec[b])
+            elif t == 203 and _zonal_active(row, outside_rhs):     # :93-107, whole block
+                q = characteristic_q_k1d(self.cfg, q, self.qref, self.kvec, self.shape)
             elif t == 401:
                 for v in range(5):                                  # sponge_layer_core.f90:80-84
                     q[..., v] = q[..., v] - self.shape * (q[..., v] - self.qref[..., v])
@@ -739,6 +799,10 @@ class Solver:
                 qs[b] = characteristic_qs_k1d(self.cfg, qs[b], q[b2], row[7:10])
             elif t == 201:
                 qs[b] = characteristic_qs_k1d(self.cfg, qs[b], q[b], row[7:10])
+            elif t == 202:                                          # boundary_conditions.f90:176-179
+                qs[b] = characteristic_qs_k1d(self.cfg, qs[b], q[b], self.kvec[b])
+            elif t == 203 and _zonal_active(row, outside_rhs):     # :181-195
+                qs = characteristic_qs_k1d(self.cfg, qs, q, self.kvec, self.shape)
             elif t == 401:
                 for v in range(5):                                  # sponge_layer_core.f90:163-165
                     qs[..., v] = qs[..., v] - self.shape * qs[..., v]
@@ -755,6 +819,10 @@ class Solver:
                 rhs[b + (comp - 1,)] = 0.0
             elif t == 204:
                 rhs[b] = characteristic_rhs_k1d(self.cfg, rhs[b], q[b], self.qref[b], row[7:10])
+            elif t == 205:                                          # boundary_conditions.f90:272-274
+                rhs[b] = characteristic_rhs_k1d(self.cfg, rhs[b], q[b], self.qref[b], self.kvec[b])
+            elif t == 206:                                          # :276-279, whole block
+                rhs = characteristic_rhs_k1d(self.cfg, rhs, q, self.qref, self.kvec, self.shape)
             elif t == 400:                                          # sponge_layer_core.f90:45-48
                 for v in range(5):
                     rhs[..., v] = rhs[..., v] - self.shape * (q[..., v] - self.qref[..., v])

@@ -262,6 +262,8 @@ def rhs_interior_vjp(S: O.Solver, q: np.ndarray, lam: np.ndarray) -> np.ndarray:
 
 def rhs_vjp(S: O.Solver, q_in: np.ndarray, lam: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
     """(d rhs_direct/d q)^T lam at q_in, and the cotangent of the forcing (d rhs/d f)^T lam."""
+    if any(int(round(r[0])) in (202, 203, 205, 206) for r in S.bc):
+        raise NotImplementedError("the zonal BC types are not transposed")
     _, qb = bc_q_vjp(S, q_in, np.zeros_like(q_in))
     lam_pre, lam_qb = bc_rhs_vjp(S, qb, lam)
     lam_qb = lam_qb + rhs_interior_vjp(S, qb, lam_pre)

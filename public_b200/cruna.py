@@ -38,7 +38,7 @@ DIFF = {"empty": 0, "o2_e_c_o": 1, "o4_e_c_p": 2, "o4_e_c_o": 3, "o4_i_c_p_pade"
 FILTER = {"empty": 0, "o2_i_c_p": 1, "o6_i_c_p": 2, "o2_i_c_o": 3, "o4_i_c_o": 4, "o6_i_c_o": 5,
           "o8_i_c_o": 6, "o10_i_c_o": 7, "o10_e_c_p": 8}
 PRECISION = {"fp64": 0, "fp32": 1}
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 ERRORS = {-1: "CRUNA_ERR_ARG", -2: "CRUNA_ERR_CUDA", -3: "CRUNA_ERR_NOMEM", -4: "CRUNA_ERR_STATE",
           -5: "CRUNA_ERR_UNSUPPORTED", -6: "CRUNA_ERR_NODEVICE"}
@@ -58,7 +58,7 @@ class _Config(C.Structure):
         ("gamma", C.c_double), ("R", C.c_double), ("W", C.c_double), ("mu0", C.c_double),
         ("T0", C.c_double), ("Pr", C.c_double), ("dt", C.c_double), ("heat_flux_dx", C.c_int32),
         ("precision", C.c_int32), ("sponge_length", C.c_double * 3), ("sponge_amplitude", C.c_double),
-        ("sponge_shape", C.c_int32), ("device", C.c_int32), ("check_every", C.c_int32),
+        ("sponge_shape", C.c_int32), ("device", C.c_int32), ("check_every", C.c_int32), ("kvector", C.c_int32),
     ]
 
 
@@ -189,6 +189,7 @@ class Settings:
     bc: Optional[np.ndarray] = None
     device: int = 0
     check_every: int = 0
+    kvector: str = "diagonal"
 
     @classmethod
     def from_dict(cls, d: dict) -> "Settings":
@@ -223,6 +224,7 @@ class Settings:
         c.sponge_shape = 0 if self.sponge_shape == "quadratic" else 1
         c.device = int(self.device)
         c.check_every = int(self.check_every)
+        c.kvector = {"diagonal": 0, "orthogonal": 1, "hedgehog": 2}[self.kvector]
         return c
 
 

@@ -401,9 +401,22 @@ int cruna_init(const cruna_config *cfg, const double *bc_table, int nbc, cruna_c
           c->has_q_bc = true;
           c->has_sponge = true;
           break;
+        case 202:  // characteristic on q with the normal-vector field, on the row's box
+        case 203:  // zonal: the whole block, weighted by the sponge shape (boundary_conditions.f90:93-107)
+        case 205:  // as 202 on the RHS
+        case 206:  // as 203 on the RHS
+          if (b.type == 203 || b.type == 206) {
+            b.is = 0; b.ie = cfg->n[0] - 1; b.js = 0; b.je = cfg->n[1] - 1; b.ks = 0; b.ke = cfg->n[2] - 1;
+            b.only = b.type == 203 ? (int)std::lround(r[7]) : 0;  // -1 outside_rhs_only, 1 inside_rhs_only
+          }
+          if (cfg->kvector < 0 || cfg->kvector > 2) fail(c, CRUNA_ERR_ARG, "kvector must be 0, 1 or 2");
+          if (b.type <= 203) c->has_q_bc = true;
+          else c->has_rhs_bc = true;
+          if (!c->kvec) c->kvec = dalloc(c, (size_t)c->g.N * 3);
+          break;
         default:
           fail(c, CRUNA_ERR_UNSUPPORTED, "boundary type " + std::to_string(b.type) +
-                                             " is not available (supported: 0,100,200,201,204,400,401)");
+                                             " is not available (supported: 0,100,200-206,400,401)");
       }
       c->bc.push_back(b);
     }
@@ -438,6 +451,7 @@ int cruna_init(const cruna_config *cfg, const double *bc_table, int nbc, cruna_c
       c->sponge.szp = upload(c, f[2][1]);
       c->sponge.amp = cfg->sponge_amplitude;
     }
+    if (c->kvec) build_kvector(c);
     // reference state defaults to zero until cruna_set_reference
     c->qref = dalloc(c, (size_t)N5(c));
     CRUNA_CUDA_CHECK(cudaMemsetAsync(c->qref, 0, sizeof(double) * N5(c), c->stream));

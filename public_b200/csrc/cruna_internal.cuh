@@ -94,6 +94,7 @@ struct BCRow {
   double k[3];
   int comp;                    // wall component (0-based)
   int shift[3];                // type 200: offset of the aim plane
+  int only = 0;                // type 203: -1 applies outside the RHS only, 1 inside only
 };
 
 // device sponge-shape factors: phi = (((sx[i]*sym[j])*syp[j])*szm[k])*szp[k]; shape = amp*(1-phi)
@@ -135,6 +136,7 @@ struct cruna_ctx {
   // device memory
   std::vector<void *> allocations;
   double *qref = nullptr;        // 5N
+  double *kvec = nullptr;        // 3N boundary normal vectors (zonal BC types 202/203/205/206)
   double *force = nullptr;       // 5N or null
   double *st[6] = {nullptr};     // state-sized work buffers
   double *io[4] = {nullptr};     // staging for host-pointer entry points (5N each)
@@ -187,6 +189,7 @@ void rhs_adjoint_fused(cruna_ctx *c, const double *qs, const double *q, const do
                        int stage, const double *qs0, double *acc, double *qnext, double dt);
 bool filter_fused_supported(const cruna_ctx *c);
 void filter3_fused(cruna_ctx *c, const double *in, double *out, const int on[3]);
+void build_kvector(cruna_ctx *c);  // normal-vector field of the zonal BC types (ops.cu)
 void bc_q(cruna_ctx *c, double *q, int outside);
 void bc_qs(cruna_ctx *c, double *qs, const double *q, int outside);
 void bc_rhs(cruna_ctx *c, double *rhs, const double *q);

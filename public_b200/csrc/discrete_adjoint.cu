@@ -553,6 +553,9 @@ void ensure_vjp(cruna_ctx *c) {
     throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint transposes the FP64 operator: precision must be FP64"};
   if (c->closure_mlp) throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint does not transpose the closure"};
   if (c->halo_fn) throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint runs on one block (no z slabs)"};
+  for (const BCRow &r : c->bc)
+    if (r.type >= 202 && r.type <= 206 && r.type != 204)
+      throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint does not transpose the zonal BC types 202/203/205/206"};
   for (int d = 0; d < 3; ++d) {
     build_transpose(c, c->dop[d], c->dhf[d], c->dopT[d]);
     build_transpose(c, c->fop[d], c->fhf[d], c->fopT[d]);

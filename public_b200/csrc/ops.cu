@@ -137,40 +137,13 @@ __global__ void k_char_qs(Box b, Grid g, double k1, double k2, double k3, double
     int i, j, k;
     const long long p = box_point(b, g, t, i, j, k);
     const long long N = g.N, pq = p + q_off;
-    const double ds0 = -qs[p], ds1 = -qs[p + N], ds2 = -qs[p + 2 * N], ds3 = -qs[p + 3 * N],
-                 ds4 = -qs[p + 4 * N];
-    const double kx = -k1, ky = -k2, kz = -k3;
-    const double gm1 = gamma - 1.0;
-    const double c = sqrt(gamma * (q[pq + 4 * N] / q[pq]));
-    const double g_c = gm1 / c;
-    const double u = q[pq + N] / q[pq], v = q[pq + 2 * N] / q[pq], w = q[pq + 3 * N] / q[pq];
-    const double ku = kx * u + ky * v + kz * w;
-    const double kus = kx * ds1 + ky * ds2 + kz * ds3;
-    const double ruus = (ds0 + u * ds1 + v * ds2 + w * ds3) / c;
-    const double rups = ruus + ds4 / g_c;
-    double drs = 0.0, dus = 0.0, dvs = 0.0, dws = 0.0, dps = 0.0;
-    if (ku < 0.0) {
-      drs = ds0 + ku * kus;
-      dus = ds1 - kx * kus;
-      dvs = ds2 - ky * kus;
-      dws = ds3 - kz * kus;
-      dps = -g_c * ruus;
+    double sv[5], qv[5], out[5];
+    for (int v = 0; v < 5; ++v) {
+      sv[v] = qs[p + v * N];
+      qv[v] = q[pq + v * N];
     }
-    if (ku + c < 0.0) {
-      const double tmp = 0.5 * (kus + rups);
-      drs = drs - ku * tmp; dus = dus + kx * tmp; dvs = dvs + ky * tmp; dws = dws + kz * tmp;
-      dps = dps + g_c * tmp;
-    }
-    if (ku - c < 0.0) {
-      const double tmp = 0.5 * (kus - rups);
-      drs = drs - ku * tmp; dus = dus + kx * tmp; dvs = dvs + ky * tmp; dws = dws + kz * tmp;
-      dps = dps - g_c * tmp;
-    }
-    qs[p] = qs[p] + drs;
-    qs[p + N] = qs[p + N] + dus;
-    qs[p + 2 * N] = qs[p + 2 * N] + dvs;
-    qs[p + 3 * N] = qs[p + 3 * N] + dws;
-    qs[p + 4 * N] = qs[p + 4 * N] + dps;
+    char_qs_point(sv, qv, k1, k2, k3, gamma, out);
+    for (int v = 0; v < 5; ++v) qs[p + v * N] = out[v];
   }
 }
 
@@ -192,6 +165,107 @@ __global__ void k_char_rhs(Box b, Grid g, double k1, double k2, double k3, doubl
     char_rhs_point(rv, qv, av, k1, k2, k3, gamma, dt, out);
     for (int v = 0; v < 5; ++v) rhs[p + v * N] = out[v];
   }
+}
+
+// zonal variants with a normal vector per point (nonreflecting.f90:141-233, :345-449, :558-661): types
+// 202 / 205 on their box, 203 / 206 on the whole block weighted by the sponge shape
+__global__ void k_char_q4(Box b, Grid g, const double *__restrict__ kv, SpongeDev sp, int shaped, double gamma,
+                          double *q, const double *aim) {
+  const long long tot = b.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    const long long p = box_point(b, g, t, i, j, k);
+    const long long N = g.N;
+    double qv[5], av[5], out[5];
+    for (int v = 0; v < 5; ++v) {
+      qv[v] = q[p + v * N];
+      av[v] = aim[p + v * N];
+    }
+    char_q_point(qv, av, kv[p], kv[p + N], kv[p + 2 * N], gamma, out, shaped ? sponge_at(sp, g, p) : 1.0);
+    for (int v = 0; v < 5; ++v) q[p + v * N] = out[v];
+  }
+}
+
+__global__ void k_char_qs4(Box b, Grid g, const double *__restrict__ kv, SpongeDev sp, int shaped, double gamma,
+                           double *qs, const double *q) {
+  const long long tot = b.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    const long long p = box_point(b, g, t, i, j, k);
+    const long long N = g.N;
+    double sv[5], qv[5], out[5];
+    for (int v = 0; v < 5; ++v) {
+      sv[v] = qs[p + v * N];
+      qv[v] = q[p + v * N];
+    }
+    char_qs_point(sv, qv, kv[p], kv[p + N], kv[p + 2 * N], gamma, out, shaped ? sponge_at(sp, g, p) : 1.0);
+    for (int v = 0; v < 5; ++v) qs[p + v * N] = out[v];
+  }
+}
+
+__global__ void k_char_rhs4(Box b, Grid g, const double *__restrict__ kv, SpongeDev sp, int shaped, double gamma,
+                            double dt, double *rhs, const double *q, const double *aim) {
+  const long long tot = b.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    const long long p = box_point(b, g, t, i, j, k);
+    const long long N = g.N;
+    double rv[5], qv[5], av[5], out[5];
+    for (int v = 0; v < 5; ++v) {
+      rv[v] = rhs[p + v * N];
+      qv[v] = q[p + v * N];
+      av[v] = aim[p + v * N];
+    }
+    char_rhs_point(rv, qv, av, kv[p], kv[p + N], kv[p + 2 * N], gamma, dt, out, shaped != 0,
+                   shaped ? sponge_at(sp, g, p) : 0.0);
+    for (int v = 0; v < 5; ++v) rhs[p + v * N] = out[v];
+  }
+}
+
+// boundary normal vectors (init_orthogonal_and_diagonal_kvector, init_orthogonal_kvector,
+// init_hedgehog_kvector, normalize_kvector: boundary_normal_vector.f90:37-261)
+__global__ void k_kvector(Grid g, int kind, double x00, double x01, double x02, double L0, double L1, double L2,
+                          double dx0, double dx1, double dx2, double *kv) {
+  const long long N = g.N;
+  const double half = 0.5 * fmin(fmin(dx0 / L0, dx1 / L1), dx2 / L2);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x) {
+    const long long i = p % g.n1, j = (p / g.n1) % g.n2, k = p / ((long long)g.n1 * g.n2);
+    const double X[3] = {x00 + (g.n1 > 1 ? (double)i * dx0 : 0.0), x01 + (g.n2 > 1 ? (double)j * dx1 : 0.0),
+                         x02 + (g.n3 > 1 ? (double)k * dx2 : 0.0)};
+    const double Lv[3] = {L0, L1, L2};
+    double kk[3];
+    for (int d = 0; d < 3; ++d) kk[d] = X[d] - (x00 * (d == 0) + x01 * (d == 1) + x02 * (d == 2) + 0.5 * Lv[d]);
+    bool normalize = true;
+    if (kind != 2) {
+      for (int d = 0; d < 3; ++d) kk[d] = kk[d] / Lv[d];
+      const double a[3] = {fabs(kk[0]), fabs(kk[1]), fabs(kk[2])};
+      const double m = fmax(fmax(a[0], a[1]), a[2]);
+      const int dom = (m == a[0]) ? 0 : ((m == a[1]) ? 1 : 2);
+      for (int d = 0; d < 3; ++d) {
+        if (d == dom) kk[d] = copysign(1.0, kk[d]);
+        else if (kind == 0 && m - a[d] < half) kk[d] = copysign(1.0, kk[d]);
+        else kk[d] = 0.0;
+      }
+      normalize = (kind == 0);
+    }
+    if (normalize) {
+      const double r = sqrt(kk[0] * kk[0] + kk[1] * kk[1] + kk[2] * kk[2]);
+      for (int d = 0; d < 3; ++d) kk[d] = kk[d] / r;
+    }
+    for (int d = 0; d < 3; ++d) kv[p + d * N] = kk[d];
+  }
+}
+
+void build_kvector(cruna_ctx *c) {
+  const double L[3] = {c->cfg.x1[0] - c->cfg.x0[0], c->cfg.x1[1] - c->cfg.x0[1], c->cfg.x1[2] - c->cfg.x0[2]};
+  k_kvector<<<(int)std::min<long long>(nblocks(c->g.N), 148LL * 32), kThreads, 0, c->stream>>>(
+      c->g, c->cfg.kvector, c->cfg.x0[0], c->cfg.x0[1], c->cfg.x0[2], L[0], L[1], L[2], c->dx[0], c->dx[1],
+      c->dx[2], c->kvec);
+  CRUNA_LAUNCH_CHECK(c);
 }
 
 // wall_slip_no_thermodynamics (src/boundaries/wall_boundary_conditions.f90:13-23)
@@ -236,7 +310,7 @@ __global__ void k_sponge(int mode, Grid g, SpongeDev sp, double gamma, double *a
   }
 }
 
-void bc_q(cruna_ctx *c, double *q, int /*outside*/) {
+void bc_q(cruna_ctx *c, double *q, int outside) {
   for (const BCRow &r : c->bc) {
     Box b = box_of(r);
     const int blocks = nblocks(b.count());
@@ -252,11 +326,15 @@ void bc_q(cruna_ctx *c, double *q, int /*outside*/) {
       k_sponge<<<nblocks(c->g.N), kThreads, 0, c->stream>>>(1, c->g, c->sponge, c->cfg.gamma, q, nullptr,
                                                              c->qref);
       CRUNA_LAUNCH_CHECK(c);
+    } else if (r.type == 202 || (r.type == 203 && (outside ? r.only != 1 : r.only != -1))) {
+      k_char_q4<<<blocks, kThreads, 0, c->stream>>>(b, c->g, c->kvec, c->sponge, r.type == 203, c->cfg.gamma, q,
+                                                    c->qref);
+      CRUNA_LAUNCH_CHECK(c);
     }
   }
 }
 
-void bc_qs(cruna_ctx *c, double *qs, const double *q, int /*outside*/) {
+void bc_qs(cruna_ctx *c, double *qs, const double *q, int outside) {
   for (const BCRow &r : c->bc) {
     Box b = box_of(r);
     const int blocks = nblocks(b.count());
@@ -268,6 +346,10 @@ void bc_qs(cruna_ctx *c, double *qs, const double *q, int /*outside*/) {
     } else if (r.type == 401) {
       k_sponge<<<nblocks(c->g.N), kThreads, 0, c->stream>>>(2, c->g, c->sponge, c->cfg.gamma, qs, nullptr,
                                                              nullptr);
+      CRUNA_LAUNCH_CHECK(c);
+    } else if (r.type == 202 || (r.type == 203 && (outside ? r.only != 1 : r.only != -1))) {
+      k_char_qs4<<<blocks, kThreads, 0, c->stream>>>(b, c->g, c->kvec, c->sponge, r.type == 203, c->cfg.gamma, qs,
+                                                     q);
       CRUNA_LAUNCH_CHECK(c);
     }
   }
@@ -286,6 +368,10 @@ void bc_rhs(cruna_ctx *c, double *rhs, const double *q) {
     } else if (r.type == 400) {
       k_sponge<<<nblocks(c->g.N), kThreads, 0, c->stream>>>(0, c->g, c->sponge, c->cfg.gamma, rhs, q,
                                                              c->qref);
+      CRUNA_LAUNCH_CHECK(c);
+    } else if (r.type == 205 || r.type == 206) {
+      k_char_rhs4<<<nblocks(b.count()), kThreads, 0, c->stream>>>(b, c->g, c->kvec, c->sponge, r.type == 206,
+                                                                 c->cfg.gamma, c->cfg.dt, rhs, q, c->qref);
       CRUNA_LAUNCH_CHECK(c);
     }
   }
