@@ -299,6 +299,19 @@ int cruna_closure_features_dev(cruna_ctx *ctx, const double *q, double delta, fl
    MLP must outlive the attachment; the discrete adjoint (mode 1) is unavailable while attached. */
 int cruna_set_closure(cruna_ctx *ctx, cruna_mlp *mlp, double delta);
 
+/* Optimisation loop of cruna.f90:78-179 on a time-constant forcing f (5 fields, updated in place):
+   per loop the direct run and J (J_hist[loop-1]); except in the last loop the gradient dJ/df
+   (cruna_gradient with the context's adjoint mode, nsnap snapshots), for loop >= ls_start the
+   quadratic line search of ls_quadratic_fit (line_search.f90:23-127: J at alpha0/2 and alpha0, dgesv
+   of [alpha^2, alpha, 1], alpha = -b/2a capped at 10 alpha0, alpha0 when singular; alpha_hist), and
+   update_force as steepest descent f <- f - alpha dJ/df (force.f90:76-81 leaves the update to the
+   case).  The context's own forcing is restored afterwards.  J_hist (maxloop) and alpha_hist
+   (maxloop - 1) are host arrays and may be NULL. */
+int cruna_optimize(cruna_ctx *ctx, const double *q0, const cruna_objective *obj, int nsteps, int nsnap,
+                   int maxloop, int ls_start, double alpha0, double *f, double *J_hist, double *alpha_hist);
+int cruna_optimize_dev(cruna_ctx *ctx, const double *q0, const cruna_objective *obj, int nsteps, int nsnap,
+                       int maxloop, int ls_start, double alpha0, double *f, double *J_hist, double *alpha_hist);
+
 /* State check used by the run loops: returns CRUNA_ERR_STATE if any rho <= 0, p <= 0 or a
    non-finite value is found in q (device pointer). */
 int cruna_check_state_dev(cruna_ctx *ctx, const double *q);

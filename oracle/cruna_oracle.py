@@ -1095,7 +1095,7 @@ def gradient_store_all(S: "Solver", q0: np.ndarray, steps: int, objective: dict)
     """J, dJ/df (time-constant forcing) and dJ/dq0 with the whole trajectory stored.
 
     objective = {"kind": "plane_p2", "normal": d, "index": i, "p_inf": p} gives
-    J = sum_{nt=1..steps} dt * j(Q(nt)) with the adjoint source g(Q(nt)) at adjoint step nt (the
+    J = sum_{nt=1..steps} dt * j(Q(nt)) with the adjoint source -dj/dq(Q(nt)) at adjoint step nt (the
     order of computation_adjoint.f90:66-81); {"kind": "kinetic_energy"} gives J = E(Q(steps)) with
     qs(T) = dE/dq.  dJ/df = integral of qs dt (trapezoid over the adjoint trajectory), dJ/dq0 = qs(0).
     """
@@ -1106,7 +1106,8 @@ def gradient_store_all(S: "Solver", q0: np.ndarray, steps: int, objective: dict)
     gfn = None
     if objective["kind"] == "plane_p2":
         def gfn(qq, nt):
-            return objective_plane_p2(cfg, qq, objective["normal"], objective["index"], objective["p_inf"])[1]
+            # rk_o4_e.f90:62-105 integrates dqs/dt = rhs_adjoint + g backwards: g = -dj/dq makes qs ~ dJ/dq
+            return -objective_plane_p2(cfg, qq, objective["normal"], objective["index"], objective["p_inf"])[1]
         for nt in range(1, steps + 1):
             J += cfg.dt * objective_plane_p2(cfg, Q[nt], objective["normal"], objective["index"],
                                              objective["p_inf"])[0]

@@ -358,3 +358,46 @@ def gradient_discrete(S: O.Solver, q0: np.ndarray, steps: int, objective: dict):
             J += cfg.dt * j
             lam = lam + cfg.dt * g
     return J, np.asfortranarray(gf), np.asfortranarray(lam)
+
+
+# ------------------------------------------------------------------------------------------------
+# optimisation loop of cruna.f90:78-179 with ls_quadratic_fit (line_search.f90:23-127)
+# ------------------------------------------------------------------------------------------------
+def optimize(S: O.Solver, q0: np.ndarray, steps: int, objective: dict, maxloop: int, ls_start: int,
+             alpha0: float, f0: np.ndarray, discrete: bool = False):
+    """Steepest descent on the time-constant forcing f: per loop the direct run and J, then (except in
+    the last loop) the adjoint gradient, the quadratic line search over alpha in {0, alpha0/2, alpha0}
+    (two more direct runs, dgesv of [alpha^2, alpha, 1] c = J; alpha = -c1 / (2 c0), capped at
+    10 alpha0, alpha0 when the system is singular), and f <- f - alpha dJ/df.
+    Returns (J per loop, alpha per loop except the last, final f)."""
+    f = np.asfortranarray(f0.copy())
+    Js, alphas = [], []
+    for loop in range(1, maxloop + 1):
+        S.force = f
+        if loop == maxloop:
+            Js.append(objective_value(S, q0, steps, objective))
+            break
+        if discrete:
+            J, gf, _ = gradient_discrete(S, q0, steps, objective)
+        else:
+            J, gf, _ = O.gradient_store_all(S, q0, steps, objective)
+        Js.append(J)
+        alpha = alpha0
+        if loop >= ls_start:
+            a = np.array([0.0, 0.5, 1.0]) * alpha0
+            Jl = [J]
+            for ls in (1, 2):
+                S.force = np.asfortranarray(f - a[ls] * gf)
+                Jl.append(objective_value(S, q0, steps, objective))
+            M = np.stack([a ** 2, a, np.ones(3)], axis=1)
+            try:
+                coef = np.linalg.solve(M, np.array(Jl))
+                alpha = -coef[1] / (2.0 * coef[0])
+                if alpha > 10.0 * alpha0:
+                    alpha = 10.0 * alpha0
+            except np.linalg.LinAlgError:
+                alpha = alpha0
+        alphas.append(alpha)
+        f = np.asfortranarray(f - alpha * gf)
+    S.force = f
+    return np.array(Js), np.array(alphas), f

@@ -128,6 +128,8 @@ _SIGNATURES = {
     "cruna_closure_features_dev": (_I, [_P, _P, C.c_double, _P]),
     "cruna_set_closure": (_I, [_P, _P, C.c_double]),
     "cruna_set_halo_exchange": (_I, [_P, _P, _P]),
+    "cruna_optimize": (_I, [_P, _P, C.POINTER(Objective), _I, _I, _I, _I, C.c_double, _P, _P, _P]),
+    "cruna_optimize_dev": (_I, [_P, _P, C.POINTER(Objective), _I, _I, _I, _I, C.c_double, _P, _P, _P]),
     "cruna_set_adjoint_mode": (_I, [_P, _I]),
     "cruna_rhs_direct_vjp": (_I, [_P, _P, _P, _P, _P]),
     "cruna_rhs_direct_vjp_dev": (_I, [_P, _P, _P, _P, _P]),
@@ -450,6 +452,18 @@ class Cruna:
         """Install a z-slab halo callback (a ctypes function of public_b200.slabs.HALO_FN; None detaches)."""
         self._check(self.lib.cruna_set_halo_exchange(self.h, None if fn is None else C.cast(fn, C.c_void_p), None))
         self._halo_fn = fn
+
+    def optimize(self, q0, objective: Objective, nsteps: int, nsnap: int, maxloop: int, ls_start: int,
+                 alpha0: float, f0):
+        """Optimisation loop of cruna.f90 on the forcing: returns (J per loop, alpha per loop, final f)."""
+        a = self._state(q0)
+        f = np.array(self._state(f0), order="F", copy=True)
+        Jh = np.zeros(maxloop)
+        ah = np.zeros(max(maxloop - 1, 1))
+        self._check(self.lib.cruna_optimize(self.h, _ptr(a), C.byref(objective), int(nsteps), int(nsnap),
+                                            int(maxloop), int(ls_start), float(alpha0), _ptr(f), _ptr(Jh),
+                                            _ptr(ah)))
+        return Jh, ah[:maxloop - 1], f
 
     def set_adjoint_mode(self, mode: int):
         """0: the reference's continuous adjoint (default); 1: the exact discrete adjoint."""

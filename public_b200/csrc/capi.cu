@@ -554,7 +554,7 @@ int cruna_set_reference(cruna_ctx *c, const double *qref) {
 }
 
 // the forcing the kernels add: the caller's, or (with a closure) the closure's buffer, which adds it
-void point_forcing(cruna_ctx *c, double *user) {
+static void point_forcing(cruna_ctx *c, double *user) {
   if (c->closure_mlp) c->user_force = user;
   else c->force = user;
 }
@@ -847,6 +847,9 @@ void adjoint_loop_step(cruna_ctx *c, double *qs, const double *q0, const double 
 
 long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
                         double *J_dev, double *grad_f, double *grad_q0, std::vector<void *> &scratch);
+double objective_direct_impl(cruna_ctx *c, const double *q0, int nsteps, const cruna_objective *obj,
+                             std::vector<void *> &scratch);
+void axpy_state(cruna_ctx *c, double a, const double *x, double *y);
 
 }  // namespace cruna
 
@@ -958,6 +961,148 @@ static int gradient_common(cruna_ctx *c, const double *q0_dev, int nsteps, int n
   for (void *q : scratch) cudaFree(q);
   if (direct_steps) *direct_steps = adv;
   return CRUNA_OK;
+}
+
+// optimisation loop of cruna.f90:78-179 on the device-resident forcing f (5N, updated in place):
+// direct run and J, adjoint gradient (except in the last loop), ls_quadratic_fit
+// (line_search.f90:23-127) when loop >= ls_start, update f <- f - alpha dJ/df
+static int optimize_common(cruna_ctx *c, const double *q0, const cruna_objective *obj, int nsteps, int nsnap,
+                           int maxloop, int ls_start, double alpha0, double *f, double *J_hist,
+                           double *alpha_hist) {
+  if (!q0 || !obj || !f || maxloop < 1 || nsteps < 1 || nsnap < 1 || !(alpha0 > 0.0))
+    fail(c, CRUNA_ERR_ARG, "bad arguments to cruna_optimize");
+  if (c->halo_fn) fail(c, CRUNA_ERR_UNSUPPORTED, "objective reductions over z slabs are not provided");
+  if (obj->kind == CRUNA_OBJ_PLANE_P2 &&
+      (obj->normal < 1 || obj->normal > 3 || obj->index < 1 || obj->index > c->cfg.n[obj->normal - 1]))
+    fail(c, CRUNA_ERR_ARG, "bad objective plane");
+  if (obj->kind != CRUNA_OBJ_PLANE_P2 && obj->kind != CRUNA_OBJ_KINETIC_ENERGY)
+    fail(c, CRUNA_ERR_ARG, "unknown objective kind");
+  std::vector<void *> scratch;
+  double *saved_user = c->closure_mlp ? c->user_force : c->force;
+  try {
+    auto alloc = [&]() {
+      void *p = nullptr;
+      CRUNA_CUDA_CHECK(cudaMalloc(&p, sizeof(double) * N5(c)));
+      scratch.push_back(p);
+      return static_cast<double *>(p);
+    };
+    double *gf = alloc(), *fb = alloc(), *Jd = nullptr;
+    {
+      void *p = nullptr;
+      CRUNA_CUDA_CHECK(cudaMalloc(&p, sizeof(double)));
+      scratch.push_back(p);
+      Jd = static_cast<double *>(p);
+    }
+    for (int loop = 1; loop <= maxloop; ++loop) {
+      point_forcing(c, f);
+      double J = 0.0;
+      if (loop == maxloop) {                                   // cruna.f90:127-133: stop after the objective
+        std::vector<void *> sc;
+        try {
+          J = objective_direct_impl(c, q0, nsteps, obj, sc);
+        } catch (...) {
+          for (void *p : sc) cudaFree(p);
+          throw;
+        }
+        for (void *p : sc) cudaFree(p);
+        if (J_hist) J_hist[loop - 1] = J;
+        break;
+      }
+      std::vector<void *> sc;
+      try {
+        gradient_impl(c, q0, nsteps, nsnap, obj, Jd, gf, nullptr, sc);
+      } catch (...) {
+        for (void *p : sc) cudaFree(p);
+        throw;
+      }
+      for (void *p : sc) cudaFree(p);
+      CRUNA_CUDA_CHECK(cudaMemcpyAsync(&J, Jd, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+      if (J_hist) J_hist[loop - 1] = J;
+      double alpha = alpha0;
+      if (loop >= ls_start) {                                  // ls_quadratic_fit
+        const double a[3] = {0.0, 0.5 * alpha0, alpha0};
+        double Js[3] = {J, 0.0, 0.0};
+        copy_state(c, fb, f, 5);                               // backup_force
+        for (int ls = 1; ls <= 2; ++ls) {
+          copy_state(c, f, fb, 5);
+          axpy_state(c, -a[ls], gf, f);                        // update_force with alpha = a[ls]
+          std::vector<void *> s2;
+          try {
+            Js[ls] = objective_direct_impl(c, q0, nsteps, obj, s2);
+          } catch (...) {
+            for (void *p : s2) cudaFree(p);
+            throw;
+          }
+          for (void *p : s2) cudaFree(p);
+        }
+        copy_state(c, f, fb, 5);                               // restore_force
+        // dgesv of M c = Js, M rows (a^2, a, 1): Gaussian elimination with partial pivoting
+        double M[3][4];
+        for (int i = 0; i < 3; ++i) {
+          M[i][0] = a[i] * a[i];
+          M[i][1] = a[i];
+          M[i][2] = 1.0;
+          M[i][3] = Js[i];
+        }
+        bool singular = false;
+        for (int col = 0; col < 3 && !singular; ++col) {
+          int piv = col;
+          for (int r = col + 1; r < 3; ++r)
+            if (std::fabs(M[r][col]) > std::fabs(M[piv][col])) piv = r;
+          if (M[piv][col] == 0.0) {
+            singular = true;
+            break;
+          }
+          if (piv != col)
+            for (int k = 0; k < 4; ++k) std::swap(M[piv][k], M[col][k]);
+          for (int r = col + 1; r < 3; ++r) {
+            const double m = M[r][col] / M[col][col];
+            for (int k = col; k < 4; ++k) M[r][k] -= m * M[col][k];
+          }
+        }
+        if (!singular) {
+          double x[3];
+          for (int i = 2; i >= 0; --i) {
+            double s = M[i][3];
+            for (int k = i + 1; k < 3; ++k) s -= M[i][k] * x[k];
+            x[i] = s / M[i][i];
+          }
+          alpha = -x[1] / (2.0 * x[0]);
+          if (alpha > 10.0 * alpha0) alpha = 10.0 * alpha0;     // line_search.f90:103-112
+        }
+      }
+      if (alpha_hist) alpha_hist[loop - 1] = alpha;
+      axpy_state(c, -alpha, gf, f);                            // update_force
+    }
+    CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  } catch (...) {
+    cudaStreamSynchronize(c->stream);
+    for (void *p : scratch) cudaFree(p);
+    point_forcing(c, saved_user);
+    throw;
+  }
+  for (void *p : scratch) cudaFree(p);
+  point_forcing(c, saved_user);
+  return CRUNA_OK;
+}
+
+int cruna_optimize_dev(cruna_ctx *c, const double *q0, const cruna_objective *obj, int nsteps, int nsnap,
+                       int maxloop, int ls_start, double alpha0, double *f, double *J_hist, double *alpha_hist) {
+  return guarded(c, [&]() -> int {
+    return optimize_common(c, q0, obj, nsteps, nsnap, maxloop, ls_start, alpha0, f, J_hist, alpha_hist);
+  });
+}
+
+int cruna_optimize(cruna_ctx *c, const double *q0, const cruna_objective *obj, int nsteps, int nsnap, int maxloop,
+                   int ls_start, double alpha0, double *f, double *J_hist, double *alpha_hist) {
+  return guarded(c, [&]() -> int {
+    if (!q0 || !f) fail(c, CRUNA_ERR_ARG, "null pointer");
+    double *dq = stage_in(c, 0, q0, 5), *df = stage_in(c, 1, f, 5);
+    int rc = optimize_common(c, dq, obj, nsteps, nsnap, maxloop, ls_start, alpha0, df, J_hist, alpha_hist);
+    stage_out(c, f, df, 5);
+    return rc;
+  });
 }
 
 int cruna_set_halo_exchange(cruna_ctx *c, int (*fn)(void *, double *, int, void *), void *user) {

@@ -13,7 +13,8 @@
 //
 // Objectives (the reference leaves them to each case, src/opt/objective.f90:19-45):
 //   plane_p2:        J = sum_{nt=1..T} dt * sum_plane w (p - p_inf)^2, adjoint source
-//                    g = (0,0,0,0, 2 w (p - p_inf)) on the plane (calc_objective_g)
+//                    g = -dj/dq = (0,0,0,0, -2 w (p - p_inf)) on the plane (calc_objective_g; the sign makes
+//                    the backward-integrated qs an approximation of dJ/dq)
 //   kinetic_energy:  J = sum dV |rho u|^2 / (2 rho) at t_T, qs(T) = dJ/dq(T)
 // Gradients (calc_grad, force.f90:41-45): dJ/df for a time-constant forcing added to the RHS is the
 // time integral of qs (trapezoid over the adjoint trajectory), dJ/dq0 = qs(0).
@@ -77,7 +78,7 @@ void build_schedule(int n, int S, std::vector<int> &kbest, long long &cost_out) 
 
 // ---- objective kernels (deterministic two-level sums) --------------------------------------------
 __global__ void k_plane_obj(Grid g, int normal, int index, double w, double p_inf, const double *q, double *gsrc,
-                            double *partial) {
+                            double *partial, double gsign) {
   __shared__ double sh[RB];
   const long long n1 = g.n1, n2 = g.n2, n3 = g.n3;
   const long long na = normal == 0 ? n2 : n1, nb = normal == 2 ? n2 : n3;
@@ -92,7 +93,7 @@ __global__ void k_plane_obj(Grid g, int normal, int index, double w, double p_in
     const long long p = i + n1 * (j + n2 * k);
     const double dp = q[p + 4 * g.N] - p_inf;
     acc += w * dp * dp;
-    gsrc[p + 4 * g.N] = 2.0 * w * dp;
+    gsrc[p + 4 * g.N] = gsign * (2.0 * w * dp);
   }
   sh[threadIdx.x] = acc;
   __syncthreads();
@@ -190,7 +191,7 @@ struct GradientRun {
     double w = 1.0;
     for (int d = 0; d < 3; ++d)
       if (d != nd && c->cfg.n[d] > 1) w *= c->dx[d];
-    k_plane_obj<<<RG, RB, 0, c->stream>>>(c->g, nd, obj->index - 1, w, obj->p_inf, q, gsrc, partial);
+    k_plane_obj<<<RG, RB, 0, c->stream>>>(c->g, nd, obj->index - 1, w, obj->p_inf, q, gsrc, partial, 1.0);
     CRUNA_LAUNCH_CHECK(c);
     k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, c->cfg.dt, 1);
     CRUNA_LAUNCH_CHECK(c);
@@ -248,7 +249,9 @@ struct GradientRun {
       double w = 1.0;
       for (int d = 0; d < 3; ++d)
         if (d != nd && c->cfg.n[d] > 1) w *= c->dx[d];
-      k_plane_obj<<<RG, RB, 0, c->stream>>>(c->g, nd, obj->index - 1, w, obj->p_inf, qnt, gsrc, partial);
+      // CRUNA's adjoint stepper integrates dqs/dt = rhs_adjoint(qs) + g backwards (rk_o4_e.f90:62-105),
+      // so qs approximates dJ/dq when the source is g = -dj/dq
+      k_plane_obj<<<RG, RB, 0, c->stream>>>(c->g, nd, obj->index - 1, w, obj->p_inf, qnt, gsrc, partial, -1.0);
       CRUNA_LAUNCH_CHECK(c);
       k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, dt, 1);
       CRUNA_LAUNCH_CHECK(c);
@@ -330,6 +333,55 @@ long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, c
   }
   if (grad_q0) copy_state(c, grad_q0, g.qs, 5);
   return g.advanced;
+}
+
+// J of the direct loop from q0 alone (calc_direct + calc_objective, cruna.f90:90-117): the line search's
+// objective evaluations
+double objective_direct_impl(cruna_ctx *c, const double *q0, int nsteps, const cruna_objective *obj,
+                             std::vector<void *> &scratch) {
+  auto alloc = [&](size_t b) {
+    void *p = nullptr;
+    CRUNA_CUDA_CHECK(cudaMalloc(&p, b));
+    scratch.push_back(p);
+    return static_cast<double *>(p);
+  };
+  const size_t bytes = sizeof(double) * (size_t)c->g.N * 5;
+  double *work = alloc(bytes), *gsrc = alloc(bytes), *partial = alloc(sizeof(double) * (RG + 1)),
+         *J = alloc(sizeof(double));
+  CRUNA_CUDA_CHECK(cudaMemsetAsync(J, 0, sizeof(double), c->stream));
+  copy_state(c, work, q0, 5);
+  const bool plane = obj->kind == CRUNA_OBJ_PLANE_P2;
+  const int nd = obj->normal - 1;
+  double w = 1.0, dV = 1.0;
+  for (int d = 0; d < 3; ++d) {
+    if (c->cfg.n[d] > 1) dV *= c->dx[d];
+    if (d != nd && c->cfg.n[d] > 1) w *= c->dx[d];
+  }
+  for (int nt = 1; nt <= nsteps; ++nt) {
+    direct_loop_step(c, work, nt);
+    if (plane) {
+      k_plane_obj<<<RG, RB, 0, c->stream>>>(c->g, nd, obj->index - 1, w, obj->p_inf, work, gsrc, partial, 1.0);
+      CRUNA_LAUNCH_CHECK(c);
+      k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, c->cfg.dt, 1);
+      CRUNA_LAUNCH_CHECK(c);
+    }
+  }
+  if (!plane) {
+    k_ke_obj<<<RG, RB, 0, c->stream>>>(c->g, dV, work, nullptr, partial);
+    CRUNA_LAUNCH_CHECK(c);
+    k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, 1.0, 0);
+    CRUNA_LAUNCH_CHECK(c);
+  }
+  double h = 0.0;
+  CRUNA_CUDA_CHECK(cudaMemcpyAsync(&h, J, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  return h;
+}
+
+void axpy_state(cruna_ctx *c, double a, const double *x, double *y) {
+  const long long M = c->g.N * 5;
+  k_axpy<<<(int)std::min<long long>((M + 255) / 256, 148LL * 32), 256, 0, c->stream>>>(M, a, x, y, 0);
+  CRUNA_LAUNCH_CHECK(c);
 }
 
 }  // namespace cruna

@@ -125,3 +125,31 @@ def test_gradient_matches_finite_differences_mixing_layer():
     o = {"kind": "plane_p2", "normal": 2, "index": 5, "p_inf": float(q[..., 4].mean())}
     eq, ef = grad_mismatch(S, q, 3, o, eps=1e-7)
     assert eq < 1e-6 and ef < 1e-6, (eq, ef)
+
+
+@pytest.mark.parametrize("kind", ["kinetic_energy", "plane_p2"])
+def test_continuous_gradient_points_along_the_exact_one(kind):
+    """CRUNA's continuous adjoint (with the source sign -dj/dq its backward stepper needs) gives a
+    dJ/dq0 and dJ/df along the exact discrete gradient: identical for the terminal kinetic energy, within
+    a few degrees for the plane objective (whose source is a plane of delta functions)."""
+    s, q = cases.taylor_green(n=12, seed=3)
+    s["mu0"] = 0.02
+    S = O.Solver(ocfg(s), force=np.zeros_like(q))
+    o = {"kind": kind, "normal": 1, "index": 5, "p_inf": float(q[..., 4].mean())}
+    _, gfd, gqd = DA.gradient_discrete(S, q, 4, o)
+    _, gfc, gqc = O.gradient_store_all(S, q, 4, o)
+    cos = lambda a, b: float(np.sum(a * b) / np.linalg.norm(a) / np.linalg.norm(b))
+    lim = 0.9999 if kind == "kinetic_energy" else 0.97
+    assert cos(gqc, gqd) > lim and cos(gfc, gfd) > lim, (cos(gqc, gqd), cos(gfc, gfd))
+
+
+def test_optimisation_loop_reduces_the_objective():
+    s, q = cases.taylor_green(n=12, seed=3)
+    s["mu0"] = 0.02
+    S = O.Solver(ocfg(s))
+    o = {"kind": "plane_p2", "normal": 1, "index": 5, "p_inf": float(q[..., 4].mean())}
+    for discrete in (False, True):
+        Js, alphas, f = DA.optimize(S, q, 4, o, maxloop=3, ls_start=1, alpha0=10.0, f0=np.zeros_like(q),
+                                    discrete=discrete)
+        assert Js[1] < 0.5 * Js[0] and Js[2] <= Js[1] * 1.001, (discrete, Js)
+        assert np.all(alphas > 0)

@@ -179,3 +179,23 @@ def test_discrete_mode_needs_fp64():
         assert e.value.code == -5
         with pytest.raises(CrunaError):
             c.rhs_direct_vjp(q, q)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_optimisation_loop_matches_oracle(mode):
+    """cruna_optimize (cruna.f90:78-179 with ls_quadratic_fit) against the oracle's loop: the objective
+    of every loop, the line-search step sizes and the final forcing."""
+    s, q0 = cases.taylor_green(n=12, seed=3)
+    s["mu0"] = 0.02
+    S = O.Solver(ocfg(s))
+    pinf = float(np.mean(q0[..., 4]))
+    o = {"kind": "plane_p2", "normal": 1, "index": 5, "p_inf": pinf}
+    f0 = cases.smooth_random_state((12, 12, 12), seed=8, p0=0.0, rho0=0.0, amp=0.01)
+    Jr, ar, fr = DA.optimize(S, q0, 4, o, maxloop=3, ls_start=1, alpha0=10.0, f0=f0, discrete=mode == 1)
+    with Cruna(Settings.from_dict(s), force=np.zeros_like(q0)) as c:
+        c.set_adjoint_mode(mode)
+        Jg, ag, fg = c.optimize(q0, c.objective("plane_p2", normal=2, index=6, p_inf=pinf), 4, 3, 3, 1, 10.0, f0)
+    assert np.allclose(Jg, Jr, rtol=1e-10, atol=0), (Jg, Jr)
+    assert np.allclose(ag, ar, rtol=1e-7, atol=0), (ag, ar)
+    assert cot_err(fg, fr) < 1e-8, cot_err(fg, fr)
+    assert Jg[-1] < 0.5 * Jg[0]
