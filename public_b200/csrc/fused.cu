@@ -35,7 +35,7 @@ namespace {
 // plane fields: 0 u, 1 v, 2 w, 3 T', 4 p', 5 rho*u, 6 rho*v ; ring fields: 0 u, 1 v, 2 w, 3 T', 4 p', 5 rho*w
 // ------------------------------------------------------------------------------------------------
 template <typename T, int R, bool PER>
-__global__ void __launch_bounds__(TX *TY, 2) k_pass_g(const __grid_constant__ FusedArgs a) {
+__global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_pass_g(const __grid_constant__ FusedArgs a) {
   constexpr int PW = TX + 2 * R, PH = TY + 2 * R, PS = PW * PH;
   constexpr int NS = ring_slots(R);
   constexpr int NRF = 6, RS = TX * TY;
@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_pass_g(const __grid_constant__ Fu
 // plane fields: 0 t11, 1 t12, 2 t13, 3 t22, 4 t23, 5 hx, 6 hy ; ring fields: 0 t13, 1 t23, 2 t33, 3 hz
 // ------------------------------------------------------------------------------------------------
 template <typename T, int R, bool PER>
-__global__ void __launch_bounds__(TX *TY, 2) k_pass_d(const __grid_constant__ FusedArgs a) {
+__global__ void __launch_bounds__(TX *TY, 3) k_pass_d(const __grid_constant__ FusedArgs a) {
   constexpr int PW = TX + 2 * R, PH = TY + 2 * R, PS = PW * PH;
   constexpr int NS = ring_slots(R);
   constexpr int NRF = 4, RS = TX * TY;
