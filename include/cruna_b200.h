@@ -299,6 +299,12 @@ int cruna_closure_features_dev(cruna_ctx *ctx, const double *q, double delta, fl
    MLP must outlive the attachment; the discrete adjoint (mode 1) is unavailable while attached. */
 int cruna_set_closure(cruna_ctx *ctx, cruna_mlp *mlp, double delta);
 
+/* J of the objective after nsteps direct loop steps from q0 (calc_direct + calc_objective,
+   cruna.f90:90-117), without the adjoint: what finite-difference checks and line searches evaluate. */
+int cruna_objective_value(cruna_ctx *ctx, const double *q0, int nsteps, const cruna_objective *obj, double *J);
+int cruna_objective_value_dev(cruna_ctx *ctx, const double *q0, int nsteps, const cruna_objective *obj,
+                              double *J);
+
 /* Optimisation loop of cruna.f90:78-179 on a time-constant forcing f (5 fields, updated in place):
    per loop the direct run and J (J_hist[loop-1]); except in the last loop the gradient dJ/df
    (cruna_gradient with the context's adjoint mode, nsnap snapshots), for loop >= ls_start the

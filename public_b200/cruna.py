@@ -128,6 +128,8 @@ _SIGNATURES = {
     "cruna_closure_features_dev": (_I, [_P, _P, C.c_double, _P]),
     "cruna_set_closure": (_I, [_P, _P, C.c_double]),
     "cruna_set_halo_exchange": (_I, [_P, _P, _P]),
+    "cruna_objective_value": (_I, [_P, _P, _I, C.POINTER(Objective), C.POINTER(C.c_double)]),
+    "cruna_objective_value_dev": (_I, [_P, _P, _I, C.POINTER(Objective), C.POINTER(C.c_double)]),
     "cruna_optimize": (_I, [_P, _P, C.POINTER(Objective), _I, _I, _I, _I, C.c_double, _P, _P, _P]),
     "cruna_optimize_dev": (_I, [_P, _P, C.POINTER(Objective), _I, _I, _I, _I, C.c_double, _P, _P, _P]),
     "cruna_set_adjoint_mode": (_I, [_P, _I]),
@@ -452,6 +454,18 @@ class Cruna:
         """Install a z-slab halo callback (a ctypes function of public_b200.slabs.HALO_FN; None detaches)."""
         self._check(self.lib.cruna_set_halo_exchange(self.h, None if fn is None else C.cast(fn, C.c_void_p), None))
         self._halo_fn = fn
+
+    def objective_value(self, q0, nsteps: int, objective: Objective) -> float:
+        J = C.c_double()
+        self._check(self.lib.cruna_objective_value(self.h, _ptr(self._state(q0)), int(nsteps), C.byref(objective),
+                                                   C.byref(J)))
+        return J.value
+
+    def objective_value_dev(self, q0_ptr: int, nsteps: int, objective: Objective) -> float:
+        J = C.c_double()
+        self._check(self.lib.cruna_objective_value_dev(self.h, C.c_void_p(q0_ptr), int(nsteps), C.byref(objective),
+                                                       C.byref(J)))
+        return J.value
 
     def optimize(self, q0, objective: Objective, nsteps: int, nsnap: int, maxloop: int, ls_start: int,
                  alpha0: float, f0):

@@ -1087,6 +1087,35 @@ static int optimize_common(cruna_ctx *c, const double *q0, const cruna_objective
   return CRUNA_OK;
 }
 
+int cruna_objective_value_dev(cruna_ctx *c, const double *q0, int nsteps, const cruna_objective *obj, double *J) {
+  return guarded(c, [&]() -> int {
+    if (!q0 || !obj || !J || nsteps < 1) fail(c, CRUNA_ERR_ARG, "bad arguments to cruna_objective_value");
+    if (c->halo_fn) fail(c, CRUNA_ERR_UNSUPPORTED, "objective reductions over z slabs are not provided");
+    if (obj->kind == CRUNA_OBJ_PLANE_P2 &&
+        (obj->normal < 1 || obj->normal > 3 || obj->index < 1 || obj->index > c->cfg.n[obj->normal - 1]))
+      fail(c, CRUNA_ERR_ARG, "bad objective plane");
+    if (obj->kind != CRUNA_OBJ_PLANE_P2 && obj->kind != CRUNA_OBJ_KINETIC_ENERGY)
+      fail(c, CRUNA_ERR_ARG, "unknown objective kind");
+    std::vector<void *> sc;
+    try {
+      *J = objective_direct_impl(c, q0, nsteps, obj, sc);
+    } catch (...) {
+      for (void *p : sc) cudaFree(p);
+      throw;
+    }
+    for (void *p : sc) cudaFree(p);
+    return CRUNA_OK;
+  });
+}
+
+int cruna_objective_value(cruna_ctx *c, const double *q0, int nsteps, const cruna_objective *obj, double *J) {
+  return guarded(c, [&]() -> int {
+    if (!q0) fail(c, CRUNA_ERR_ARG, "null pointer");
+    double *dq = stage_in(c, 0, q0, 5);
+    return cruna_objective_value_dev(c, dq, nsteps, obj, J);
+  });
+}
+
 int cruna_optimize_dev(cruna_ctx *c, const double *q0, const cruna_objective *obj, int nsteps, int nsnap,
                        int maxloop, int ls_start, double alpha0, double *f, double *J_hist, double *alpha_hist) {
   return guarded(c, [&]() -> int {

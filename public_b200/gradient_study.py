@@ -1,0 +1,113 @@
+"""Adjoint-gradient study on the temporal mixing layer (the mixing-layer configuration with adjoint).
+
+Objective: J = sum over the direct steps of dt * integral over the plane y = y_plane of (p - p_inf)^2 dA
+(y_plane measured from the lower boundary of the 60-high box, 5 below the layer's centre by default)
+(computed on the device, ``cruna_objective_value``); control: a time-constant forcing of the pressure
+equation (the fifth RHS component).  For both adjoints the library offers -- the reference's
+continuous inviscid adjoint (mode 0) and the exact discrete adjoint (mode 1) -- the gradient comes from
+``cruna_gradient`` with binomial checkpointing in ``nsnap`` HBM snapshots, and is checked against
+central finite differences of J on ``ndir`` random directions (seed 2).
+
+The mixing layer has type-201 characteristic boundaries, which switch waves on the sign of v at the
+y boundaries: J is only piecewise smooth, so a difference step must be small enough that no boundary
+point changes branch; the study reports the comparison at two steps (``--eps``, default 1e-6 and
+1e-7).
+
+    python -m public_b200.gradient_study [--n 128 96 64] [--steps 200] [--nsnap 64] [--ndir 16]
+        [--eps 1e-6 1e-7] [--json out.json]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+
+def run(args) -> dict:
+    import torch
+
+    from . import cases
+    from .cruna import Cruna, Settings
+
+    dev = torch.device("cuda", 0)
+    n = tuple(args.n)
+    s, q0 = cases.mixing_layer(n=n)
+    L_y = s["x1"][1] - s["x0"][1]
+    dy = L_y / (n[1] - 1)
+    j_plane = int(round(args.y_plane / dy)) + 1       # 1-based index, distance from the lower y boundary
+    p_inf = float(np.mean(q0[..., 4]))
+    N = int(np.prod(n))
+    q = torch.from_numpy(np.ascontiguousarray(q0.ravel(order="F"))).to(dev)
+    f = torch.zeros(5 * N, dtype=torch.float64, device=dev)
+    gf = torch.empty_like(f)
+    out = {"workload": f"mixing layer {n[0]}x{n[1]}x{n[2]}, {args.steps} steps, plane y={args.y_plane} "
+                       f"from the lower boundary (index {j_plane}), pressure-equation forcing, {args.nsnap} snapshots",
+           "ndir": args.ndir}
+    rng = np.random.Generator(np.random.PCG64(2))
+    dirs = []
+    for _ in range(args.ndir):
+        d = np.zeros((N, 5))
+        d[:, 4] = rng.standard_normal(N)
+        dirs.append(torch.from_numpy(np.ascontiguousarray(d.T.ravel())).to(dev))
+    with Cruna(Settings.from_dict(s), qref=q0, force=np.zeros_like(q0)) as c:
+        obj = c.objective("plane_p2", normal=2, index=j_plane, p_inf=p_inf)
+        c.set_forcing_dev(f.data_ptr())
+        J0 = c.objective_value_dev(q.data_ptr(), args.steps, obj)
+        out["J"] = J0
+        fd = {}
+        t0 = time.time()
+        for eps in args.eps:
+            vals = []
+            for d in dirs:
+                fp = f + eps * d
+                c.set_forcing_dev(fp.data_ptr())
+                Jp = c.objective_value_dev(q.data_ptr(), args.steps, obj)
+                fm = f - eps * d
+                c.set_forcing_dev(fm.data_ptr())
+                Jm = c.objective_value_dev(q.data_ptr(), args.steps, obj)
+                vals.append((Jp - Jm) / (2 * eps))
+            fd[eps] = np.array(vals)
+        out["fd_seconds"] = time.time() - t0
+        c.set_forcing_dev(f.data_ptr())
+        for mode in (0, 1):
+            c.set_adjoint_mode(mode)
+            torch.cuda.synchronize()
+            t0 = time.time()
+            J, adv = c.gradient_dev(q.data_ptr(), args.steps, args.nsnap, obj, gf.data_ptr(), None)
+            c.sync()
+            secs = time.time() - t0
+            g5 = gf.view(5, N)[4]
+            ad = np.array([float((g5 * d.view(5, N)[4]).sum().item()) for d in dirs])
+            key = "continuous" if mode == 0 else "discrete"
+            res = {"J": J, "direct_steps": adv, "seconds": secs}
+            for eps, v in fd.items():
+                rel = np.abs(ad - v) / np.maximum(np.abs(v), 1e-300)
+                res[f"fd_rel_err_eps{eps:g}"] = {"median": float(np.median(rel)), "max": float(np.max(rel))}
+                res[f"cosine_eps{eps:g}"] = float(np.dot(ad, v) / (np.linalg.norm(ad) * np.linalg.norm(v)))
+            out[key] = res
+        c.set_adjoint_mode(0)
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--n", type=int, nargs=3, default=[128, 96, 64])
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--nsnap", type=int, default=64)
+    ap.add_argument("--ndir", type=int, default=16)
+    ap.add_argument("--y-plane", type=float, default=25.0)
+    ap.add_argument("--eps", type=float, nargs="+", default=[1e-6, 1e-7])
+    ap.add_argument("--json", type=str, default=None)
+    args = ap.parse_args(argv)
+    res = run(args)
+    line = json.dumps(res)
+    print(line)
+    if args.json:
+        with open(args.json, "w") as fh:
+            fh.write(line + "\n")
+
+
+if __name__ == "__main__":
+    main()
