@@ -82,56 +82,49 @@ __global__ void __launch_bounds__(FTHR) k_filter_xy(const __grid_constant__ Filt
       xf[c] = a.on[0] ? filt(a, p, 1) : p[0];
     }
     __syncthreads();
-    for (int c = tid; c < FXT * FYT; c += FTHR) {
-      const int lx = c % FXT, ly = c / FXT;
-      const int gi = i0 + lx, gj = j0 + ly;
-      if (gi < a.g.n1 && gj < a.g.n2) {
-        const double *p = xf + (ly + FR) * FXT + lx;
-        out[gi + n1 * gj + kofs] = a.on[1] ? filt(a, p, FXT) : p[0];
+    {  // y filter: each thread takes a column and FYT / 8 consecutive rows from a register window
+      constexpr int RPT = FYT / (FTHR / FXT), NW = RPT + 2 * FR;
+      const int lx = tid % FXT, ly0 = (tid / FXT) * RPT;
+      double w[NW];
+#pragma unroll
+      for (int m = 0; m < NW; ++m) w[m] = xf[(ly0 + m) * FXT + lx];
+#pragma unroll
+      for (int r = 0; r < RPT; ++r) {
+        const int gi = i0 + lx, gj = j0 + ly0 + r;
+        if (gi < a.g.n1 && gj < a.g.n2) out[gi + n1 * gj + kofs] = a.on[1] ? filt(a, w + r + FR, 1) : w[r + FR];
       }
     }
     __syncthreads();
   }
 }
 
-// pass 2: z filter with per-thread register queues of 2*FR+1 planes for the five variables, the next
-// plane loaded one step ahead
+// pass 2: z filter, one variable per block (blockIdx.z = chunk * 5 + variable) with a per-thread
+// register queue of 2*FR+1 planes, the next plane loaded one step ahead
 __global__ void __launch_bounds__(FTHR) k_filter_z(const __grid_constant__ FilterArgs a) {
   constexpr int NQ = 2 * FR + 1;
   const int i = blockIdx.x * 32 + threadIdx.x % 32, j = blockIdx.y * 8 + threadIdx.x / 32;
   if (i >= a.g.n1 || j >= a.g.n2) return;
-  const int k0 = blockIdx.z * a.kc, k1 = min(k0 + a.kc, a.g.n3);
+  const int v = blockIdx.z % 5, chunk = blockIdx.z / 5;
+  const int k0 = chunk * a.kc, k1 = min(k0 + a.kc, a.g.n3);
   const long long N = a.g.N, n12 = (long long)a.g.n1 * a.g.n2;
-  const long long col = i + (long long)a.g.n1 * j;
+  const long long col = i + (long long)a.g.n1 * j + v * N;
   const int n3 = a.n[2];
   const double *in = a.in + col;
   double *out = a.out + col;
-  double q[5][NQ], nx[5];
+  constexpr int PD = 4;  // planes in flight ahead of the queue
+  double q[NQ], nx[PD];
 #pragma unroll
-  for (int m = 0; m < NQ - 1; ++m) {
-    const long long o = n12 * wrapi(k0 - FR + m, n3);
+  for (int m = 0; m < NQ - 1; ++m) q[m] = in[n12 * wrapi(k0 - FR + m, n3)];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) q[v][m] = in[v * N + o];
-  }
-  {
-    const long long o = n12 * wrapi(k0 + FR, n3);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) nx[v] = in[v * N + o];
-  }
+  for (int d = 0; d < PD; ++d) nx[d] = (k0 + d < k1) ? in[n12 * wrapi(k0 + FR + d, n3)] : 0.0;
   for (int k = k0; k < k1; ++k) {
+    q[NQ - 1] = nx[0];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) q[v][NQ - 1] = nx[v];
-    if (k + 1 < k1) {
-      const long long o = n12 * wrapi(k + 1 + FR, n3);
+    for (int d = 0; d < PD - 1; ++d) nx[d] = nx[d + 1];
+    if (k + PD < k1) nx[PD - 1] = in[n12 * wrapi(k + PD + FR, n3)];
+    out[n12 * k] = filt(a, q + FR, 1);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) nx[v] = in[v * N + o];
-    }
-#pragma unroll
-    for (int v = 0; v < 5; ++v) out[v * N + n12 * k] = filt(a, q[v] + FR, 1);
-#pragma unroll
-    for (int v = 0; v < 5; ++v)
-#pragma unroll
-      for (int m = 0; m < NQ - 1; ++m) q[v][m] = q[v][m + 1];
+    for (int m = 0; m < NQ - 1; ++m) q[m] = q[m + 1];
   }
 }
 
@@ -193,11 +186,11 @@ void filter3_fused(cruna_ctx *c, const double *in, double *out, const int on_in[
     a.out = out;
     const int zx = (c->g.n1 + 31) / 32, zy = (c->g.n2 + 7) / 8;
     const int n3 = c->g.n3;
-    int nz = std::max(1, std::min(std::max(1, n3 / 16), (8 * 148 + zx * zy - 1) / (zx * zy)));
+    int nz = std::max(1, std::min(std::max(1, n3 / 32), (16 * 148 + 5 * zx * zy - 1) / (5 * zx * zy)));
     a.kc = (n3 + nz - 1) / nz;
     nz = (n3 + a.kc - 1) / a.kc;
     ProfScope ps(c, "filter_z");
-    k_filter_z<<<dim3(zx, zy, nz), FTHR, 0, c->stream>>>(a);
+    k_filter_z<<<dim3(zx, zy, 5 * nz), FTHR, 0, c->stream>>>(a);
     CRUNA_LAUNCH_CHECK(c);
   }
 }
