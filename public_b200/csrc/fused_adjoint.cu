@@ -23,6 +23,7 @@ struct AdjArgs {
   DirOpF op[3];
   int kc;
   double gamma;
+  double p_ref;        // FP32 stencils: pressure offset differenced instead of p (0 in FP64)
   const double *qs;    // stage input (5 fields)
   const double *q;     // frozen direct state (5 fields)
   const double *src;   // adjoint source g (5 fields) or null
@@ -70,10 +71,11 @@ __device__ __forceinline__ void adj_dir(int d, double u1, double u2, double u3, 
   }
 }
 
-// plane fields: 0..4 qs1..qs5, 5 p, 6 u, 7 v ; column fields: 0..4 qs1..qs5, 5 p, 6 w
-template <int R, bool PER>
-__global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ AdjArgs a) {
-  using T = double;
+// plane fields: 0..4 qs1..qs5, 5 p - p_ref, 6 u, 7 v ; column fields: 0..4 qs1..qs5, 5 p - p_ref, 6 w.
+// T is the type of the shared-memory fields and of the derivatives (double, or float for the
+// FP32-stencil precision); the assembly and the RK update stay in double.
+template <typename T, int R, bool PER>
+__global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_adj_pass(const __grid_constant__ AdjArgs a) {
   constexpr int PW = TX + 2 * R, PH = TY + 2 * R, PS = PW * PH;
   constexpr int NS = ring_slots(R);
   constexpr int NPF = 8, NRF = 7, RS = TX * TY;
@@ -100,9 +102,9 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
     // v8: qs1..qs5, rho, rho*w, p
     T *rp = ring + (((kk % NS) + NS) % NS) * NRF * RS + tid;
 #pragma unroll
-    for (int f = 0; f < 5; ++f) rp[f * RS] = v8[f];
-    rp[5 * RS] = v8[7];
-    rp[6 * RS] = v8[6] * (1.0 / v8[5]);
+    for (int f = 0; f < 5; ++f) rp[f * RS] = T(v8[f]);
+    rp[5 * RS] = T(v8[7] - a.p_ref);
+    rp[6 * RS] = T(v8[6] * (1.0 / v8[5]));
   };
   auto load8 = [&](long long pt, double *v8) {
     v8[0] = S0[pt]; v8[1] = S1[pt]; v8[2] = S2[pt]; v8[3] = S3[pt]; v8[4] = S4[pt];
@@ -117,7 +119,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
   }
   // register prefetch of the ring plane k+R+1 and the centre (rho, rho*u, rho*v) of plane k+1
   double pf[8];
-  double pc[3] = {1.0, 0.0, 0.0};
+  double pc[4] = {1.0, 0.0, 0.0, 1.0};
   int pf_ok = 0;
   auto prefetch = [&](int kk, int kc) {
     const int gk = gidx(oz, kk);
@@ -128,6 +130,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
       pc[0] = Q0[pt];
       pc[1] = Q1[pt];
       pc[2] = Q2[pt];
+      pc[3] = Q4[pt];
     }
   };
   prefetch(k0 + R, k0);
@@ -147,7 +150,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
   for (int k = k0; k < k1; ++k) {
     if (pf_ok) put_ring(k + R, pf);
     const int slot = k % NS;
-    const double rho_c = pc[0];
+    const double rho_c = pc[0], p_c = pc[3];
     const double ir = 1.0 / rho_c;                            // ns_rho_rhou_p.f90:294
     const double u1 = pc[1] * ir, u2 = pc[2] * ir;
     {
@@ -155,8 +158,8 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
       const T *rp = ring + slot * NRF * RS + tid;
 #pragma unroll
       for (int f = 0; f < 6; ++f) c[f * PS] = rp[f * RS];
-      c[6 * PS] = u1;
-      c[7 * PS] = u2;
+      c[6 * PS] = T(u1);
+      c[7 * PS] = T(u2);
     }
     const long long kofs = (long long)n12 * k;
     // epilogue inputs of this plane, issued before the barrier so their latency overlaps the stencils
@@ -180,12 +183,12 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
     for (int h = 0; h < NHT; ++h) {
       if (hs.goff[h] < 0) continue;
       T *c = plane + hs.cell[h];
-      c[0 * PS] = hv[h][0]; c[1 * PS] = hv[h][1]; c[2 * PS] = hv[h][2]; c[3 * PS] = hv[h][3];
-      c[4 * PS] = hv[h][4];
+      c[0 * PS] = T(hv[h][0]); c[1 * PS] = T(hv[h][1]); c[2 * PS] = T(hv[h][2]); c[3 * PS] = T(hv[h][3]);
+      c[4 * PS] = T(hv[h][4]);
       const double hir = 1.0 / hv[h][5];
-      c[5 * PS] = hv[h][8];
-      c[6 * PS] = hv[h][6] * hir;
-      c[7 * PS] = hv[h][7] * hir;
+      c[5 * PS] = T(hv[h][8] - a.p_ref);
+      c[6 * PS] = T(hv[h][6] * hir);
+      c[7 * PS] = T(hv[h][7] * hir);
     }
     prefetch(k + R + 1, k + 1);
     if (k + 1 < k1) halo_fetch(k + 1);
@@ -199,7 +202,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
       const double qs5 = c[4 * PS];
       const double gm1 = a.gamma - 1.0;
       const double u3 = ring[so[R] + 6 * RS];
-      const double gpr = a.gamma * c[5 * PS] / (rho_c * gm1);   // :293
+      const double gpr = a.gamma * p_c / (rho_c * gm1);         // :293
       double r1 = 0.0, r2 = 0.0, r3 = 0.0, r4 = 0.0, r5 = 0.0;  // :296
       {
         const double s = ox.scale;
@@ -271,17 +274,17 @@ __global__ void __launch_bounds__(TX *TY, 2) k_adj_pass(const __grid_constant__ 
   }
 }
 
-template <int R>
+template <typename T, int R>
 size_t smem_adj() {
-  return sizeof(double) * (8 * (TX + 2 * R) * (TY + 2 * R) + ring_slots(R) * 7 * TX * TY);
+  return sizeof(T) * (8 * (TX + 2 * R) * (TY + 2 * R) + ring_slots(R) * 7 * TX * TY);
 }
 
-template <int R, bool PER>
+template <typename T, int R, bool PER>
 void launch_adj(cruna_ctx *c, AdjArgs &a) {
   static bool configured = false;
   if (!configured) {
-    CRUNA_CUDA_CHECK(cudaFuncSetAttribute(k_adj_pass<R, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem_adj<R>()));
+    CRUNA_CUDA_CHECK(cudaFuncSetAttribute(k_adj_pass<T, R, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem_adj<T, R>()));
     configured = true;
   }
   const int bx = (c->g.n1 + TX - 1) / TX, by = (c->g.n2 + TY - 1) / TY;
@@ -292,7 +295,7 @@ void launch_adj(cruna_ctx *c, AdjArgs &a) {
   nz = (n3 + kc - 1) / kc;
   a.kc = kc;
   ProfScope ps(c, "adj_pass");
-  k_adj_pass<R, PER><<<dim3(bx, by, nz), dim3(TX, TY), smem_adj<R>(), c->stream>>>(a);
+  k_adj_pass<T, R, PER><<<dim3(bx, by, nz), dim3(TX, TY), smem_adj<T, R>(), c->stream>>>(a);
   CRUNA_LAUNCH_CHECK(c);
 }
 
@@ -307,8 +310,19 @@ void rhs_adjoint_fused(cruna_ctx *c, const double *qs_in, const double *q, const
     bc_qs(c, c->st[4], q, 0);
     qs = c->st[4];
   }
+  const bool fp32 = c->cfg.precision == CRUNA_FP32_STENCIL;
+  if (fp32 && !c->refs_set) {  // the pressure offset of the FP32 stencils (as the direct passes)
+    double h[2] = {0.0, 1.0};
+    CRUNA_CUDA_CHECK(cudaMemcpyAsync(&h[0], q + 4 * c->g.N, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CRUNA_CUDA_CHECK(cudaMemcpyAsync(&h[1], q, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+    c->p_ref = h[0];
+    c->T_ref = c->cfg.W / c->cfg.R * h[0] / h[1];
+    c->refs_set = true;
+  }
   AdjArgs a;
   a.g = c->g;
+  a.p_ref = fp32 ? c->p_ref : 0.0;
   for (int d = 0; d < 3; ++d) a.op[d] = to_dir(c->dop[d], c->dx[d], true);
   a.gamma = c->cfg.gamma;
   a.qs = qs;
@@ -326,12 +340,20 @@ void rhs_adjoint_fused(cruna_ctx *c, const double *qs_in, const double *q, const
   const int Rl = R <= 2 ? 2 : 4;
   bool per = true;
   for (int d = 0; d < 3; ++d) per = per && c->dop[d].kind == OP_STENCIL && c->dop[d].periodic && c->dop[d].r == Rl;
-  if (Rl == 2) {
-    if (per) launch_adj<2, true>(c, a);
-    else launch_adj<2, false>(c, a);
+  if (fp32) {
+    if (Rl == 2) {
+      if (per) launch_adj<float, 2, true>(c, a);
+      else launch_adj<float, 2, false>(c, a);
+    } else {
+      if (per) launch_adj<float, 4, true>(c, a);
+      else launch_adj<float, 4, false>(c, a);
+    }
+  } else if (Rl == 2) {
+    if (per) launch_adj<double, 2, true>(c, a);
+    else launch_adj<double, 2, false>(c, a);
   } else {
-    if (per) launch_adj<4, true>(c, a);
-    else launch_adj<4, false>(c, a);
+    if (per) launch_adj<double, 4, true>(c, a);
+    else launch_adj<double, 4, false>(c, a);
   }
   if (stage == 0 || split) {
     if (c->has_rhs_bc) bc_rhss(c, rhs, qs, nullptr);                // :518 (without q)
