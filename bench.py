@@ -189,10 +189,11 @@ def run_ours(args):
     s, q0 = cases.taylor_green(n=args.n, seed=rank)
     s["ai_freq"] = (1, 1, 1)
     slabs = None
-    if world > 1:
+    if world > 1 or args.slabs:
         # z slabs: the global grid is n x n x (n * world) (the Taylor-Green field repeated along z, each
         # slab with its own density noise); each rank holds n^3 interior points plus H = 2R = 8 halo
-        # planes per side, refreshed through NCCL point-to-point before every z-reading pass
+        # planes per side, refreshed through NCCL point-to-point before every z-reading pass (--slabs on
+        # one GPU: the same path, the single slab exchanging with itself)
         from public_b200.slabs import ZSlabs
         L = s["x1"][2] - s["x0"][2]
         slabs = ZSlabs((args.n, args.n, args.n * world), halo=8, rank=rank, world=world)
@@ -308,8 +309,10 @@ def run_ours(args):
         "config": {"workload": f"taylor-green {args.n}^3 Mach 0.1 Re 1600: o8 FD, o10 explicit filter every "
                                f"step, RK4 direct step + continuous-adjoint RK4 step",
                    "points": N, "parallelism": (f"z slabs x{world}: n x n x {args.n * world} global grid, "
-                                                 f"8 halo planes per side, NCCL point-to-point exchange")
-                   if world > 1 else "single GPU",
+                                                 f"8 halo planes per side, "
+                                                 + ("NCCL point-to-point exchange" if world > 1
+                                                    else "exchange of the single slab with itself"))
+                   if slabs is not None else "single GPU",
                    "l2": f"inputs ({bytes_state / 1e6:.0f} MB per state) larger than L2; no flush",
                    "precision": args.precision, "rhs_path": ctx.rhs_path},
         "direct": {"value": N * args.steps / (t_dir / 1e3), "unit": UNIT, "ms_per_step": t_dir / args.steps},
@@ -358,6 +361,8 @@ def main():
     ap.add_argument("--ref-n", type=int, default=96)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--slabs", action="store_true",
+                    help="z-slab decomposition with halo exchange also on one GPU (the path --gpus N runs)")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the host-buffer run (grids whose staging would not fit beside the device working set)")
     args = ap.parse_args()
