@@ -352,6 +352,17 @@ int cruna_rhs_direct_noalloc(const cruna_config *cfg, const double *q, double *r
 int cruna_profile_enable(cruna_ctx *ctx, int on);
 int cruna_profile_report(cruna_ctx *ctx, char *buf, int buflen);
 
+/* Step graphs: inside one call of cruna_run_direct*, cruna_run_adjoint*, cruna_gradient*,
+   cruna_objective_value* or cruna_optimize*, a loop step (time step, boundary update and the filters
+   due at that step) that repeats with the same buffers and filter pattern is recorded once as a CUDA
+   graph on the context's stream and replayed after that; the first step of each kind runs eagerly.
+   Results are bit-identical to eager launches.  Graphs are on by default and off while kernel timing
+   or a halo exchange is set; a capture the runtime refuses turns them off for the rest of the call
+   and the step runs eagerly.  cruna_graph_stats returns the counts of captures and of replays since
+   the context was created (either pointer may be NULL). */
+int cruna_set_graphs(cruna_ctx *ctx, int on);
+int cruna_graph_stats(cruna_ctx *ctx, int64_t *captured, int64_t *replayed);
+
 /* The library's restatement of LAPACK dgttrf / dgttrs('N', nrhs=1), which every compact core of the
    reference calls (e.g. diff_pen_core_o6_i_c_p.f90:135,213,219); exported so callers and tests can
    compare its factors with their LAPACK.  ipiv is 1-based as in LAPACK. */

@@ -114,6 +114,8 @@ _SIGNATURES = {
     "cruna_kernel_launches": (C.c_int64, [_P]),
     "cruna_profile_enable": (_I, [_P, _I]),
     "cruna_profile_report": (_I, [_P, C.c_char_p, _I]),
+    "cruna_set_graphs": (_I, [_P, _I]),
+    "cruna_graph_stats": (_I, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "cruna_rhs_direct_noalloc": (_I, [C.POINTER(_Config), _P, _P, _P, C.c_char_p, _I]),
     "cruna_mlp_create": (_I, [_I, C.c_uint64, C.POINTER(_P)]),
     "cruna_mlp_free": (None, [_P]),
@@ -543,6 +545,16 @@ class Cruna:
         self._check(self.lib.cruna_run_adjoint_dev(self.h, C.c_void_p(qs_ptr), C.c_void_p(Q_ptr),
                                                    None if g_ptr is None else C.c_void_p(g_ptr),
                                                    int(nt_end), int(nsteps)))
+
+    def set_graphs(self, on: bool = True):
+        """Record repeating loop steps as CUDA graphs inside run / gradient calls (default on)."""
+        self._check(self.lib.cruna_set_graphs(self.h, 1 if on else 0))
+
+    def graph_stats(self) -> Tuple[int, int]:
+        """(graphs captured, graph replays) since the context was created."""
+        cap, rep = C.c_int64(0), C.c_int64(0)
+        self._check(self.lib.cruna_graph_stats(self.h, C.byref(cap), C.byref(rep)))
+        return int(cap.value), int(rep.value)
 
     def profile(self, on: bool = True):
         self._check(self.lib.cruna_profile_enable(self.h, 1 if on else 0))

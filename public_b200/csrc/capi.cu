@@ -811,8 +811,7 @@ namespace cruna {
 
 // one step of the loop body of calc_direct (computation_direct.f90:76-95): time_stepper_direct,
 // set_boundary_condition_q(outside_rhs) and the filters whose frequency divides nt; q in place
-void direct_loop_step(cruna_ctx *c, double *q, int nt) {
-  const int on[3] = {due(c->cfg.di_freq[0], nt), due(c->cfg.di_freq[1], nt), due(c->cfg.di_freq[2], nt)};
+static void direct_loop_body(cruna_ctx *c, double *q, const int on[3]) {
   if (c->filter_fused_ok && !c->force_generic && (on[0] || on[1] || on[2])) {
     step_direct(c, q, c->st[5]);
     if (c->has_q_bc) bc_q(c, c->st[5], 1);
@@ -829,8 +828,7 @@ void direct_loop_step(cruna_ctx *c, double *q, int nt) {
 
 // one step of the loop body of calc_adjoint (computation_adjoint.f90:81-101): time_stepper_adjoint
 // with the frozen direct state q0 and source g, set_boundary_condition_qs(outside_rhs), filters
-void adjoint_loop_step(cruna_ctx *c, double *qs, const double *q0, const double *g, int nt) {
-  const int on[3] = {due(c->cfg.ai_freq[0], nt), due(c->cfg.ai_freq[1], nt), due(c->cfg.ai_freq[2], nt)};
+static void adjoint_loop_body(cruna_ctx *c, double *qs, const double *q0, const double *g, const int on[3]) {
   if (c->filter_fused_ok && !c->force_generic && (on[0] || on[1] || on[2])) {
     step_adjoint(c, qs, q0, g, c->st[5]);
     if (c->has_q_bc) bc_qs(c, c->st[5], q0, 1);
@@ -845,6 +843,19 @@ void adjoint_loop_step(cruna_ctx *c, double *qs, const double *q0, const double 
   }
 }
 
+// the loop steps as the run loops and the gradient call them: nt selects the filters due; a step
+// that repeats with the same buffers and filter pattern is replayed from a graph (step_graph.cu)
+void direct_loop_step(cruna_ctx *c, double *q, int nt) {
+  const int on[3] = {due(c->cfg.di_freq[0], nt), due(c->cfg.di_freq[1], nt), due(c->cfg.di_freq[2], nt)};
+  graph_step(c, on[0] | on[1] << 1 | on[2] << 2, q, nullptr, nullptr, [&]() { direct_loop_body(c, q, on); });
+}
+
+void adjoint_loop_step(cruna_ctx *c, double *qs, const double *q0, const double *g, int nt) {
+  const int on[3] = {due(c->cfg.ai_freq[0], nt), due(c->cfg.ai_freq[1], nt), due(c->cfg.ai_freq[2], nt)};
+  graph_step(c, 8 | on[0] | on[1] << 1 | on[2] << 2, qs, q0, g,
+             [&]() { adjoint_loop_body(c, qs, q0, g, on); });
+}
+
 long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
                         double *J_dev, double *grad_f, double *grad_q0, std::vector<void *> &scratch);
 double objective_direct_impl(cruna_ctx *c, const double *q0, int nsteps, const cruna_objective *obj,
@@ -857,6 +868,7 @@ extern "C" {
 
 // loop body of calc_direct (computation_direct.f90:64-107); traj is a device pointer or NULL
 static int run_direct_impl(cruna_ctx *c, double *q, int nt0, int nsteps, double *traj, bool traj_host) {
+  GraphScope graphs(c);
   for (int s = 1; s <= nsteps; ++s) {
     const int nt = nt0 + s;
     direct_loop_step(c, q, nt);
@@ -892,6 +904,7 @@ int cruna_run_direct(cruna_ctx *c, double *q_io, int nt0, int nsteps, double *tr
 // loop body of calc_adjoint (computation_adjoint.f90:60-108)
 static int run_adjoint_impl(cruna_ctx *c, double *qs, const double *Q, const double *G, int nt_end,
                             int nsteps, bool host) {
+  GraphScope graphs(c);
   const int nt_first = nt_end - nsteps + 1;
   for (int nt = nt_end; nt >= nt_first; --nt) {
     const long long off = (long long)(nt - nt_first) * N5(c);

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -103,6 +104,8 @@ struct SpongeDev {
   double amp = 0.0;
 };
 
+class StepGraphs;  // step_graph.cu
+
 }  // namespace cruna
 
 struct cruna_ctx {
@@ -164,6 +167,10 @@ struct cruna_ctx {
   double *cl_force = nullptr;      // forcing + closure stress divergence (5N)
   double *cl_tau = nullptr;        // model stresses (6N) and their derivatives (9N)
   float *cl_x = nullptr, *cl_y = nullptr;  // features (12N) and outputs (6N), point-major
+  // step graphs (step_graph.cu): the cache of the current run call, or null outside one
+  bool graphs_enabled = true;
+  cruna::StepGraphs *graphs = nullptr;
+  int64_t graph_captures = 0, graph_replays = 0;
 };
 
 namespace cruna {
@@ -198,6 +205,23 @@ void rk_stage(cruna_ctx *c, int stage, double dt, const double *k, const double 
               double *qnext);
 void copy_state(cruna_ctx *c, double *dst, const double *src, int nfields);
 int check_state(cruna_ctx *c, const double *q);
+
+// step graphs (step_graph.cu): a GraphScope makes a graph cache live for one run call (an inner scope
+// uses the outer one's); graph_step runs body() as the loop step keyed by (kind, a, b, d): eagerly at
+// the key's first sighting, recorded at its second, replayed after that
+class GraphScope {
+ public:
+  explicit GraphScope(cruna_ctx *c);
+  ~GraphScope();
+  GraphScope(const GraphScope &) = delete;
+  GraphScope &operator=(const GraphScope &) = delete;
+
+ private:
+  cruna_ctx *c_;
+  StepGraphs *own_ = nullptr;
+};
+void graph_step(cruna_ctx *c, int kind, const void *a, const void *b, const void *d,
+                const std::function<void()> &body);
 double *dalloc(cruna_ctx *c, size_t count);
 void ensure_generic(cruna_ctx *c);
 bool use_fused(const cruna_ctx *c);

@@ -290,6 +290,7 @@ void adjoint_loop_step(cruna_ctx *c, double *qs, const double *q0, const double 
 
 long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
                         double *J_dev, double *grad_f, double *grad_q0, std::vector<void *> &scratch) {
+  GraphScope graphs(c);
   GradientRun g;
   g.c = c;
   g.nsteps = nsteps;
@@ -339,6 +340,7 @@ long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, c
 // objective evaluations
 double objective_direct_impl(cruna_ctx *c, const double *q0, int nsteps, const cruna_objective *obj,
                              std::vector<void *> &scratch) {
+  GraphScope graphs(c);
   auto alloc = [&](size_t b) {
     void *p = nullptr;
     CRUNA_CUDA_CHECK(cudaMalloc(&p, b));
