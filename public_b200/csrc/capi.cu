@@ -91,6 +91,9 @@ void attach_factors(cruna_ctx *c, LineOp &op, const HostFactors &hf) {
   op.du = upload(c, hf.du);
   op.du2 = upload(c, hf.du2);
   op.ipiv = upload(c, hf.ipiv);
+  op.nopiv = 1;
+  for (size_t i = 0; i + 1 < hf.ipiv.size(); ++i)
+    if (hf.ipiv[i] != (int)i + 1) op.nopiv = 0;
   if (op.cyclic) {
     op.fbnorm = upload(c, hf.fbnorm);
     op.fbrat = hf.fbrat;

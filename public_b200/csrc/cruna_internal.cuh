@@ -39,6 +39,7 @@ struct LineOp {
   double div = 1.0;                // explicit part is divided by (h * div): 12 for o4 explicit
   int solve = 0;                   // dgttrs follows
   int cyclic = 0;                  // Sherman-Morrison correction follows
+  int nopiv = 0;                   // dgttrf interchanged no rows (ipiv[i] == i + 1 throughout)
   double blend = 0.0;              // >0: out = q - blend * (q - F q)
   double fbrat = 0.0;
   // device factor arrays (owned by the context)

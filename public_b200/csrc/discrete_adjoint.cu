@@ -125,6 +125,9 @@ void build_transpose(cruna_ctx *c, const LineOp &op, const HostFactors &hf, Line
   t.sop.du = upload_vec(c, ht.du);
   t.sop.du2 = upload_vec(c, ht.du2);
   t.sop.ipiv = upload_vec(c, ht.ipiv);
+  t.sop.nopiv = 1;
+  for (size_t i = 0; i + 1 < ht.ipiv.size(); ++i)
+    if (ht.ipiv[i] != (int)i + 1) t.sop.nopiv = 0;
 }
 
 __global__ void k_band_T(LineOpT op, Grid g, int dir, const double *__restrict__ in, double *__restrict__ out,

@@ -70,19 +70,369 @@ __global__ void k_line_solve(LineOp op, Grid g, int dir, double *__restrict__ da
   }
 }
 
+// ------------------------------------------------------------------------------------------------
+// fast line operators: the same arithmetic as k_line_stencil / k_line_solve (identical expressions in
+// identical order, so identical results), with the interior radius a compile-time constant, no
+// integer division per tap, and for compact operators along y and z the explicit part and the
+// dgttrs sweeps fused in one pass over each line
+// ------------------------------------------------------------------------------------------------
+
+// interior explicit part from values v(m) = f(i + m), m = -R..R, in explicit_part's order
+template <int R, bool ANTI, class V>
+__device__ __forceinline__ double interior_part(const LineOp &op, V v) {
+  if (ANTI) {
+    double t = op.c[1] * (v(1) - v(-1));
+#pragma unroll
+    for (int m = 2; m <= R; ++m) t = t + op.c[m] * (v(m) - v(-m));
+    return t;
+  }
+  double t = op.c[0] * v(0);
+#pragma unroll
+  for (int m = 1; m <= R; ++m) t = t + op.c[m] * (v(m) + v(-m));
+  return t;
+}
+
+// line_point's epilogue: derivative scale, filter blend, sign
+__device__ __forceinline__ double point_epilogue(const LineOp &op, double v, double q, double scale,
+                                                 double sign) {
+  if (op.antisym) v = v * scale;  // every OP_STENCIL derivative
+  if (op.blend > 0.0) v = q - op.blend * (q - v);
+  return sign * v;
+}
+
+// one thread per KB points stacked in z: x from the block's x range, j = blockIdx.y, the field and
+// the z chunk from blockIdx.z (strided).  DIR and F2 (f1 * f2 operand) are compile-time, so a chunk
+// whose taps all lie on its line (no periodic wrap, no closure row) reads them at fixed offsets from
+// one pointer; the KB results are formed before any is stored, so the loads of all KB points are in
+// flight together (and along z the shared taps are loaded once).  Other chunks take the generic path.
+template <int R, bool ANTI, int DIR, bool F2>
+__global__ void __launch_bounds__(128) k_line_stencil_r(LineOp op, Grid g, const double *__restrict__ f1,
+                                                        const double *__restrict__ f2,
+                                                        double *__restrict__ out, double scale, double sign,
+                                                        int nfields) {
+  constexpr int KB = 4;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= g.n1) return;
+  const long long n12 = (long long)g.n1 * g.n2;
+  const int j = blockIdx.y;
+  const int nkb = (g.n3 + KB - 1) / KB;
+  const int n = op.n;
+  const long long s = DIR == 0 ? 1 : (DIR == 1 ? (long long)g.n1 : n12);
+  for (int zf = blockIdx.z; zf < nkb * nfields; zf += gridDim.z) {
+    const int fld = zf / nkb, k0 = (zf - fld * nkb) * KB;
+    const long long p0 = x + (long long)g.n1 * j + n12 * k0;
+    double *o = out + (long long)fld * g.N + p0;
+    const int ilo = DIR == 0 ? x : (DIR == 1 ? j : k0), ihi = DIR == 2 ? k0 + KB - 1 : ilo;
+    const int lo = op.periodic ? 0 : op.nb, hi = op.periodic ? n - 1 : n - 1 - op.nb;
+    if (k0 + KB <= g.n3 && ilo - R >= 0 && ihi + R <= n - 1 && ilo >= lo && ihi <= hi) {
+      const double *a = f1 + (long long)fld * g.N + p0;
+      const double *b = F2 ? f2 + (long long)fld * g.N + p0 : nullptr;
+      double r[KB];
+#pragma unroll
+      for (int u = 0; u < KB; ++u) {
+        const double *au = a + u * n12;
+        const double *bu = F2 ? b + u * n12 : nullptr;
+        auto val = [&](int m) { return F2 ? au[m * s] * bu[m * s] : au[m * s]; };
+        const double v = interior_part<R, ANTI>(op, val);
+        r[u] = point_epilogue(op, v, op.blend > 0.0 ? val(0) : 0.0, scale, sign);
+      }
+#pragma unroll
+      for (int u = 0; u < KB; ++u) o[u * n12] = r[u];
+      continue;
+    }
+    const int kend = min(k0 + KB, g.n3);
+    for (int k = k0; k < kend; ++k) {
+      const long long p = p0 + (k - k0) * n12;
+      const int i = DIR == 0 ? x : (DIR == 1 ? j : k);
+      const long long base = p - (long long)i * s;
+      const double *a = f1 + (long long)fld * g.N + base;
+      const double *b = F2 ? f2 + (long long)fld * g.N + base : nullptr;
+      double v;
+      if (op.periodic) {
+        v = interior_part<R, ANTI>(op, [&](int m) {
+          int ii = i + m;
+          ii = ii < 0 ? ii + n : (ii >= n ? ii - n : ii);
+          return ldv(a, b, ii * s);
+        });
+      } else if (i >= op.nb && i < n - op.nb) {
+        v = interior_part<R, ANTI>(op, [&](int m) { return ldv(a, b, (i + m) * s); });
+      } else {
+        v = explicit_part(op, a, b, 0, s, i);
+      }
+      o[(k - k0) * n12] = point_epilogue(op, v, op.blend > 0.0 ? ldv(a, b, i * s) : 0.0, scale, sign);
+    }
+  }
+}
+
+// Compact operators along y or z: one thread per line, consecutive threads on consecutive x (every
+// load and store coalesced).  The operator's factors sit in shared memory (the same for every line).
+// EXPL: the explicit part comes from a sliding window of f over the interior (one new load per point;
+// the closure rows of open lines use explicit_part) and dgttrs's forward sweep runs on the fly;
+// otherwise the line of `out` is solved in place.  Then the backward sweep and the cyclic correction
+// over the stored forward values.  Every sweep reads its line CH points at a time and issues the next
+// chunk's loads before it works through the current one, so two chunks' loads are in flight.
+constexpr int kCompactMaxN = 1024;  // factors in shared memory: 44 bytes per line point
+
+template <int R, bool ANTI, bool EXPL, bool NOPIV>
+__global__ void __launch_bounds__(64) k_line_compact_yz(LineOp op, Grid g, int dir,
+                                                        const double *__restrict__ f1,
+                                                        const double *__restrict__ f2, double *out,
+                                                        double scale, double sign, int nfields) {
+  constexpr int CH = 8;
+  constexpr int W = 2 * R + 1;
+  extern __shared__ double cs[];
+  const int n = op.n;
+  double *s_dl = cs, *s_du = cs + n, *s_du2 = cs + 2 * n, *s_inv = cs + 3 * n, *s_fb = cs + 4 * n;
+  int *s_piv = reinterpret_cast<int *>(cs + 5 * n);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    s_dl[i] = i < n - 1 ? op.dl[i] : 0.0;
+    s_du[i] = i < n - 1 ? op.du[i] : 0.0;
+    s_du2[i] = i < n - 2 ? op.du2[i] : 0.0;
+    s_inv[i] = op.inv_d[i];
+    s_fb[i] = op.cyclic ? op.fbnorm[i] : 0.0;
+    s_piv[i] = NOPIV ? i + 1 : op.ipiv[i];
+  }
+  __syncthreads();
+  const long long n12 = (long long)g.n1 * g.n2;
+  const long long nlines = g.N / n;
+  const long long total = nlines * nfields;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long fld = t / nlines, l = t - fld * nlines;
+    long long base, s;
+    if (dir == 1) { const long long i = l % g.n1, k = l / g.n1; base = i + k * n12; s = g.n1; }
+    else { base = l; s = n12; }
+    double *o = out + fld * g.N + base;
+    double *po = o;  // o[(i - 1) * s] for the forward step at i
+    double cur = 0.0;
+    // dgttrs forward sweep (L with LAPACK's row interchanges) on the pair (i - 1, i); v = b[i]
+    auto fwd = [&](int i, double v) {
+      if (i == 0) {
+        cur = v;
+        return;
+      }
+      if (NOPIV || s_piv[i - 1] == i) {
+        *po = cur;
+        cur = v - s_dl[i - 1] * cur;
+      } else {
+        *po = v;
+        cur = cur - s_dl[i - 1] * v;
+      }
+      po += s;
+    };
+    if (EXPL) {
+      const double *a = f1 + fld * g.N + base;
+      const double *b = f2 ? f2 + fld * g.N + base : nullptr;
+      const int ib = op.periodic ? 0 : op.nb, ie = op.periodic ? n : n - op.nb;
+      for (int i = 0; i < ib; ++i)
+        fwd(i, point_epilogue(op, explicit_part(op, a, b, 0, s, i), ldv(a, b, i * s), scale, sign));
+      auto wrap = [&](int idx) { return op.periodic ? (idx < 0 ? idx + n : (idx >= n ? idx - n : idx)) : idx; };
+      double w[W];  // w[R + m] = f(i + m)
+#pragma unroll
+      for (int m = 0; m < W; ++m) w[m] = ldv(a, b, wrap(ib + m - R) * s);
+      auto step = [&](int i, double next) {  // position i from the window, then slide it by one
+        const double v = interior_part<R, ANTI>(op, [&](int m) { return w[R + m]; });
+        fwd(i, point_epilogue(op, v, w[R], scale, sign));
+#pragma unroll
+        for (int m = 0; m < W - 1; ++m) w[m] = w[m + 1];
+        w[W - 1] = next;
+      };
+      // chunk at i0 needs f(i0 + u + 1 + R), u < CH, while i0 + u + 1 < ie
+      int i0 = ib;
+      double nx[CH];
+      if (i0 + CH <= ie) {
+#pragma unroll
+        for (int u = 0; u < CH; ++u) nx[u] = (i0 + u + 1 < ie) ? ldv(a, b, wrap(i0 + u + 1 + R) * s) : 0.0;
+      }
+      for (; i0 + CH <= ie; i0 += CH) {
+        double cb[CH];
+#pragma unroll
+        for (int u = 0; u < CH; ++u) cb[u] = nx[u];
+        if (i0 + 2 * CH <= ie) {
+#pragma unroll
+          for (int u = 0; u < CH; ++u)
+            nx[u] = (i0 + CH + u + 1 < ie) ? ldv(a, b, wrap(i0 + CH + u + 1 + R) * s) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) step(i0 + u, cb[u]);
+      }
+      for (; i0 < ie; ++i0) step(i0, (i0 + 1 < ie) ? ldv(a, b, wrap(i0 + 1 + R) * s) : 0.0);
+      for (int i = ie; i < n; ++i)
+        fwd(i, point_epilogue(op, explicit_part(op, a, b, 0, s, i), ldv(a, b, i * s), scale, sign));
+    } else {
+      cur = o[0];
+      const double *pl = o + s;  // o[i0 * s]
+      int i0 = 1;
+      double nx[CH];
+      if (i0 + CH <= n) {
+#pragma unroll
+        for (int u = 0; u < CH; ++u) nx[u] = pl[(long long)u * s];
+      }
+      for (; i0 + CH <= n; i0 += CH) {
+        double cb[CH];
+#pragma unroll
+        for (int u = 0; u < CH; ++u) cb[u] = nx[u];
+        pl += CH * s;
+        if (i0 + 2 * CH <= n) {
+#pragma unroll
+          for (int u = 0; u < CH; ++u) nx[u] = pl[(long long)u * s];
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) fwd(i0 + u, cb[u]);
+      }
+      for (; i0 < n; ++i0, pl += s) fwd(i0, *pl);
+    }
+    // backward sweep with U (diagonal inverted, du, du2); po now points at o[(n - 1) * s]
+    double x2 = cur * s_inv[n - 1];
+    *po = x2;
+    const double xlast = x2;
+    double x1 = (po[-s] - s_du[n - 2] * x2) * s_inv[n - 2];  // n > 2R + 2 >= 4
+    po -= s;
+    *po = x1;
+    auto back = [&](int i, double bi) {
+      const double x0 = (bi - s_du[i] * x1 - s_du2[i] * x2) * s_inv[i];
+      po -= s;
+      *po = x0;
+      x2 = x1;
+      x1 = x0;
+    };
+    int i0 = n - 3;  // chunk at i0 reads positions i0 - u = po[-(u + 1) s]
+    double nb[CH];
+    if (i0 >= CH - 1) {
+#pragma unroll
+      for (int u = 0; u < CH; ++u) nb[u] = po[-(long long)(u + 1) * s];
+    }
+    for (; i0 >= CH - 1; i0 -= CH) {
+      double cb[CH];
+#pragma unroll
+      for (int u = 0; u < CH; ++u) cb[u] = nb[u];
+      if (i0 - CH >= CH - 1) {
+#pragma unroll
+        for (int u = 0; u < CH; ++u) nb[u] = po[-(long long)(CH + u + 1) * s];
+      }
+#pragma unroll
+      for (int u = 0; u < CH; ++u) back(i0 - u, cb[u]);
+    }
+    for (; i0 >= 0; --i0) back(i0, po[-s]);
+    if (op.cyclic) {  // Sherman-Morrison: x1 is the solution's first value, xlast its last
+      const double corr = x1 + op.fbrat * xlast;
+      for (int j0 = 0; j0 < n; j0 += CH) {
+        double bv[CH];
+#pragma unroll
+        for (int u = 0; u < CH; ++u) bv[u] = (j0 + u < n) ? o[(long long)(j0 + u) * s] : 0.0;
+#pragma unroll
+        for (int u = 0; u < CH; ++u)
+          if (j0 + u < n) o[(long long)(j0 + u) * s] = bv[u] - s_fb[j0 + u] * corr;
+      }
+    }
+  }
+}
+
+static size_t compact_smem(const LineOp &op) { return (size_t)op.n * (5 * sizeof(double) + sizeof(int)); }
+
+// the fast kernels handle interior radii 1..6 on lines longer than 2R + 2 (every periodic wrap then
+// stays within one period) whose open ends have at least R closure rows and an interior between them
+// (interior taps stay on the line)
+static bool fast_ok(const LineOp &op) {
+  return op.kind == OP_STENCIL && op.r >= 1 && op.r <= 6 && op.n > 2 * op.r + 2 &&
+         (op.periodic || (op.nb >= op.r && op.n >= 2 * op.nb + 2 * op.r + 1));
+}
+
+template <int R, bool ANTI, int DIR>
+static void launch_stencil_dir(cruna_ctx *c, const LineOp &op, const double *f1, const double *f2, double *out,
+                               double scale, double sign, int nfields) {
+  const int bx = c->g.n1 >= 128 ? 128 : (c->g.n1 >= 64 ? 64 : 32);
+  const dim3 grid((c->g.n1 + bx - 1) / bx, c->g.n2, std::min((c->g.n3 + 3) / 4 * nfields, 65535));
+  if (f2)
+    k_line_stencil_r<R, ANTI, DIR, true><<<grid, bx, 0, c->stream>>>(op, c->g, f1, f2, out, scale, sign, nfields);
+  else
+    k_line_stencil_r<R, ANTI, DIR, false><<<grid, bx, 0, c->stream>>>(op, c->g, f1, f2, out, scale, sign, nfields);
+}
+
+template <int R, bool ANTI>
+static void launch_stencil_rr(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
+                              double *out, double scale, double sign, int nfields) {
+  if (dir == 0) launch_stencil_dir<R, ANTI, 0>(c, op, f1, f2, out, scale, sign, nfields);
+  else if (dir == 1) launch_stencil_dir<R, ANTI, 1>(c, op, f1, f2, out, scale, sign, nfields);
+  else launch_stencil_dir<R, ANTI, 2>(c, op, f1, f2, out, scale, sign, nfields);
+}
+
+template <bool ANTI>
+static void launch_stencil_r(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
+                             double *out, double scale, double sign, int nfields) {
+  switch (op.r) {
+    case 1: launch_stencil_rr<1, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
+    case 2: launch_stencil_rr<2, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
+    case 3: launch_stencil_rr<3, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
+    case 4: launch_stencil_rr<4, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
+    case 5: launch_stencil_rr<5, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
+    case 6: launch_stencil_rr<6, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
+  }
+}
+
+template <bool ANTI>
+static void launch_compact_r(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
+                             double *out, double scale, double sign, int nfields) {
+  const long long lines = (c->g.N / op.n) * nfields;
+  const int blocks = nblocks(lines, 64);  // one line per thread: small blocks spread few lines over all SMs
+  switch (op.r) {
+#define CRUNA_COMPACT_CASE(RR)                                                                          \
+  case RR:                                                                                              \
+    if (op.nopiv)                                                                                       \
+      k_line_compact_yz<RR, ANTI, true, true><<<blocks, 64, compact_smem(op), c->stream>>>(op, c->g, dir, f1, f2, out,   \
+                                                                            scale, sign, nfields);     \
+    else                                                                                                \
+      k_line_compact_yz<RR, ANTI, true, false><<<blocks, 64, compact_smem(op), c->stream>>>(op, c->g, dir, f1, f2, out,  \
+                                                                             scale, sign, nfields);    \
+    break;
+    CRUNA_COMPACT_CASE(1) CRUNA_COMPACT_CASE(2) CRUNA_COMPACT_CASE(3)
+    CRUNA_COMPACT_CASE(4) CRUNA_COMPACT_CASE(5) CRUNA_COMPACT_CASE(6)
+#undef CRUNA_COMPACT_CASE
+  }
+}
+
+static const char *const kStencilNames[2][3] = {{"line_filter_x", "line_filter_y", "line_filter_z"},
+                                                {"line_diff_x", "line_diff_y", "line_diff_z"}};
+
 void launch_line_stencil(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
                          double *out, double scale, int nfields, double sign) {
-  const long long work = c->g.N * nfields;
-  const int blocks = (int)std::min<long long>(nblocks(work), 148LL * 64);
-  ProfScope ps(c, op.antisym ? "line_diff" : "line_filter");
-  k_line_stencil<<<blocks, kThreads, 0, c->stream>>>(op, c->g, dir, f1, f2, out, scale, sign, nfields);
+  ProfScope ps(c, kStencilNames[op.antisym ? 1 : 0][dir]);
+  if (fast_ok(op) && c->g.n2 <= 65535) {
+    if (op.antisym) launch_stencil_r<true>(c, op, dir, f1, f2, out, scale, sign, nfields);
+    else launch_stencil_r<false>(c, op, dir, f1, f2, out, scale, sign, nfields);
+  } else {
+    const long long work = c->g.N * nfields;
+    const int blocks = (int)std::min<long long>(nblocks(work), 148LL * 64);
+    k_line_stencil<<<blocks, kThreads, 0, c->stream>>>(op, c->g, dir, f1, f2, out, scale, sign, nfields);
+  }
   CRUNA_LAUNCH_CHECK(c);
 }
 
 void launch_line_solve(cruna_ctx *c, const LineOp &op, int dir, double *data, int nfields) {
   const long long lines = (c->g.N / op.n) * nfields;
-  ProfScope ps(c, "line_solve");
-  k_line_solve<<<nblocks(lines, 128), 128, 0, c->stream>>>(op, c->g, dir, data, nfields);
+  static const char *names[3] = {"line_solve_x", "line_solve_y", "line_solve_z"};
+  ProfScope ps(c, names[dir]);
+  if (dir > 0 && op.n >= 4 && op.n <= kCompactMaxN && op.nopiv)
+    k_line_compact_yz<1, false, false, true><<<nblocks(lines, 64), 64, compact_smem(op), c->stream>>>(op, c->g, dir, nullptr,
+                                                                                       nullptr, data, 1.0, 1.0,
+                                                                                       nfields);
+  else if (dir > 0 && op.n >= 4 && op.n <= kCompactMaxN)
+    k_line_compact_yz<1, false, false, false><<<nblocks(lines, 64), 64, compact_smem(op), c->stream>>>(op, c->g, dir, nullptr,
+                                                                                        nullptr, data, 1.0, 1.0,
+                                                                                        nfields);
+  else
+    k_line_solve<<<nblocks(lines, 128), 128, 0, c->stream>>>(op, c->g, dir, data, nfields);
+  CRUNA_LAUNCH_CHECK(c);
+}
+
+// explicit part and compact solve of op along y or z in one pass (fast_ok(op), op.solve, dir > 0)
+static void launch_line_compact(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
+                                double *out, double scale, int nfields) {
+  static const char *names[2][3] = {{"", "compact_filter_y", "compact_filter_z"},
+                                    {"", "compact_diff_y", "compact_diff_z"}};
+  ProfScope ps(c, names[op.antisym ? 1 : 0][dir]);
+  if (op.antisym) launch_compact_r<true>(c, op, dir, f1, f2, out, scale, 1.0, nfields);
+  else launch_compact_r<false>(c, op, dir, f1, f2, out, scale, 1.0, nfields);
   CRUNA_LAUNCH_CHECK(c);
 }
 
@@ -91,6 +441,10 @@ void apply_diff(cruna_ctx *c, int dir, const double *f1, const double *f2, doubl
                 int nfields) {
   const LineOp &op = c->dop[dir];
   const double scale = 1.0 / (h * op.div);
+  if (op.kind == OP_STENCIL && op.solve && dir > 0 && fast_ok(op) && op.n <= kCompactMaxN) {
+    launch_line_compact(c, op, dir, f1, f2, out, scale, nfields);
+    return;
+  }
   launch_line_stencil(c, op, dir, f1, f2, out, scale, nfields);
   if (op.kind == OP_STENCIL && op.solve) launch_line_solve(c, op, dir, out, nfields);
 }
@@ -99,8 +453,12 @@ void apply_diff(cruna_ctx *c, int dir, const double *f1, const double *f2, doubl
 void apply_filter(cruna_ctx *c, int dir, double *q, double *scratch, int nfields) {
   const LineOp &op = c->fop[dir];
   if (op.kind == OP_COPY) return;
-  launch_line_stencil(c, op, dir, q, nullptr, scratch, 1.0, nfields);
-  if (op.solve) launch_line_solve(c, op, dir, scratch, nfields);
+  if (op.kind == OP_STENCIL && op.solve && dir > 0 && fast_ok(op) && op.n <= kCompactMaxN) {
+    launch_line_compact(c, op, dir, q, nullptr, scratch, 1.0, nfields);
+  } else {
+    launch_line_stencil(c, op, dir, q, nullptr, scratch, 1.0, nfields);
+    if (op.solve) launch_line_solve(c, op, dir, scratch, nfields);
+  }
   CRUNA_CUDA_CHECK(cudaMemcpyAsync(q, scratch, sizeof(double) * c->g.N * nfields,
                                    cudaMemcpyDeviceToDevice, c->stream));
 }
@@ -311,6 +669,7 @@ __global__ void k_sponge(int mode, Grid g, SpongeDev sp, double gamma, double *a
 }
 
 void bc_q(cruna_ctx *c, double *q, int outside) {
+  ProfScope ps(c, "boundary");
   for (const BCRow &r : c->bc) {
     Box b = box_of(r);
     const int blocks = nblocks(b.count());
@@ -335,6 +694,7 @@ void bc_q(cruna_ctx *c, double *q, int outside) {
 }
 
 void bc_qs(cruna_ctx *c, double *qs, const double *q, int outside) {
+  ProfScope ps(c, "boundary");
   for (const BCRow &r : c->bc) {
     Box b = box_of(r);
     const int blocks = nblocks(b.count());
@@ -356,6 +716,7 @@ void bc_qs(cruna_ctx *c, double *qs, const double *q, int outside) {
 }
 
 void bc_rhs(cruna_ctx *c, double *rhs, const double *q) {
+  ProfScope ps(c, "boundary");
   for (const BCRow &r : c->bc) {
     Box b = box_of(r);
     if (r.type == 100) {
@@ -378,6 +739,7 @@ void bc_rhs(cruna_ctx *c, double *rhs, const double *q) {
 }
 
 void bc_rhss(cruna_ctx *c, double *rhss, const double *qs, const double *q) {
+  ProfScope ps(c, "boundary");
   for (const BCRow &r : c->bc) {
     Box b = box_of(r);
     if (r.type == 100) {
