@@ -206,8 +206,11 @@ int cruna_run_adjoint_dev(cruna_ctx *ctx, double *qs_io, const double *Q_traj, c
  *   CRUNA_OBJ_PLANE_P2       J = sum_{nt=1..T} dt * sum_{plane x_normal = index} dA (p - p_inf)^2,
  *                            adjoint source g = (0,0,0,0, 2 dA (p - p_inf)) on the plane
  *   CRUNA_OBJ_KINETIC_ENERGY J = sum dV |rho u|^2 / (2 rho) at the final time, qs(T) = dJ/dq
+ *   CRUNA_OBJ_ENSTROPHY      J = sum dV |curl u|^2 / 2 at the final time (the curl taken with the
+ *                            context's derivative operators, h = dx), qs(T) = dJ/dq (through the
+ *                            transposed operators)
  */
-enum cruna_objective_kind { CRUNA_OBJ_PLANE_P2 = 1, CRUNA_OBJ_KINETIC_ENERGY = 2 };
+enum cruna_objective_kind { CRUNA_OBJ_PLANE_P2 = 1, CRUNA_OBJ_KINETIC_ENERGY = 2, CRUNA_OBJ_ENSTROPHY = 3 };
 typedef struct cruna_objective {
   int32_t kind;       /* enum cruna_objective_kind */
   int32_t normal;     /* plane normal direction 1..3 (CRUNA_OBJ_PLANE_P2) */
@@ -215,6 +218,11 @@ typedef struct cruna_objective {
   int32_t reserved;
   double p_inf;       /* reference pressure */
 } cruna_objective;
+
+/* Volume diagnostics of a state: kinetic energy sum dV |rho u|^2 / (2 rho) and enstrophy
+   sum dV |curl u|^2 / 2 (either output pointer may be NULL); deterministic reductions. */
+int cruna_diagnostics(cruna_ctx *ctx, const double *q, double *kinetic_energy, double *enstrophy);
+int cruna_diagnostics_dev(cruna_ctx *ctx, const double *q, double *kinetic_energy, double *enstrophy);
 
 /* J, dJ/df for the time-constant forcing set by cruna_set_forcing (the time integral of the adjoint
    state, trapezoid rule) and dJ/dq0 = qs(0), from nsteps direct steps and the matching adjoint steps

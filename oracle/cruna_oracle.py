@@ -1091,13 +1091,60 @@ def objective_kinetic_energy(cfg: Config, q: np.ndarray):
     return E, g
 
 
+def cell_volume(cfg: Config) -> float:
+    """Volume element dV: product of the grid spacings of the non-collapsed directions."""
+    dx = cfg.dx()
+    dV = 1.0
+    for d in range(3):
+        if cfg.n[d] > 1:
+            dV *= dx[d]
+    return dV
+
+
+def vorticity(cfg: Config, q: np.ndarray):
+    """curl u with the solver's own derivative operators (Dx with h = dx; a collapsed direction's
+    empty core contributes zero): (D_y w - D_z v, D_z u - D_x w, D_x v - D_y u)."""
+    dx = cfg.dx()
+    rho = q[..., 0]
+    u = [np.asfortranarray(q[..., 1 + i] / rho) for i in range(3)]
+    D = lambda d, f: Dx(cfg, d, f, dx[d])
+    return (D(1, u[2]) - D(2, u[1]), D(2, u[0]) - D(0, u[2]), D(0, u[1]) - D(1, u[0])), u
+
+
+def objective_enstrophy(cfg: Config, q: np.ndarray):
+    """Z(q) = sum dV * 0.5 |curl u|^2 (discrete curl of the solver's derivative operators) and dZ/dq:
+    dZ/du = dV curl^T(omega) with the transposed line operators, then through u_i = (rho u_i) / rho."""
+    from . import discrete_adjoint as DA       # transposed operators (imported here: DA imports this module)
+    dV = cell_volume(cfg)
+    (wx, wy, wz), u = vorticity(cfg, q)
+    Z = float(np.sum(dV * 0.5 * (wx * wx + wy * wy + wz * wz)))
+    dx = cfg.dx()
+    DT = lambda d, f: DA.DT(cfg, d, np.asfortranarray(f), dx[d])
+    gu = [dV * (DT(2, wy) - DT(1, wz)), dV * (DT(0, wz) - DT(2, wx)), dV * (DT(1, wx) - DT(0, wy))]
+    rho = q[..., 0]
+    g = np.zeros_like(q)
+    g[..., 0] = -(u[0] * gu[0] + u[1] * gu[1] + u[2] * gu[2]) / rho
+    for i in range(3):
+        g[..., 1 + i] = gu[i] / rho
+    return Z, g
+
+
+def terminal_objective(cfg: Config, q: np.ndarray, kind: str):
+    """The final-time objectives: kinetic energy or enstrophy, value and gradient."""
+    if kind == "kinetic_energy":
+        return objective_kinetic_energy(cfg, q)
+    if kind == "enstrophy":
+        return objective_enstrophy(cfg, q)
+    raise ValueError(f"unknown terminal objective {kind}")
+
+
 def gradient_store_all(S: "Solver", q0: np.ndarray, steps: int, objective: dict):
     """J, dJ/df (time-constant forcing) and dJ/dq0 with the whole trajectory stored.
 
     objective = {"kind": "plane_p2", "normal": d, "index": i, "p_inf": p} gives
     J = sum_{nt=1..steps} dt * j(Q(nt)) with the adjoint source -dj/dq(Q(nt)) at adjoint step nt (the
     order of computation_adjoint.f90:66-81); {"kind": "kinetic_energy"} gives J = E(Q(steps)) with
-    qs(T) = dE/dq.  dJ/df = integral of qs dt (trapezoid over the adjoint trajectory), dJ/dq0 = qs(0).
+    qs(T) = dE/dq, {"kind": "enstrophy"} J = Z(Q(steps)) with qs(T) = dZ/dq.  dJ/df = integral of qs dt (trapezoid over the adjoint trajectory), dJ/dq0 = qs(0).
     """
     cfg = S.cfg
     qT, Q = S.calc_direct(q0, steps, store=True)
@@ -1112,7 +1159,7 @@ def gradient_store_all(S: "Solver", q0: np.ndarray, steps: int, objective: dict)
             J += cfg.dt * objective_plane_p2(cfg, Q[nt], objective["normal"], objective["index"],
                                              objective["p_inf"])[0]
     else:
-        J, qs = objective_kinetic_energy(cfg, Q[steps])
+        J, qs = terminal_objective(cfg, Q[steps], objective["kind"])
     qs_end, traj = S.calc_adjoint(qs, Q, g_fn=gfn)
     gf = 0.5 * cfg.dt * traj[steps]
     for nt in range(steps - 1, 0, -1):

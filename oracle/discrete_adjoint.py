@@ -325,8 +325,8 @@ def objective_value(S: O.Solver, q0: np.ndarray, steps: int, objective: dict) ->
         if objective["kind"] == "plane_p2":
             J += cfg.dt * O.objective_plane_p2(cfg, q, objective["normal"], objective["index"],
                                                objective["p_inf"])[0]
-    if objective["kind"] == "kinetic_energy":
-        J = O.objective_kinetic_energy(cfg, q)[0]
+    if objective["kind"] != "plane_p2":
+        J = O.terminal_objective(cfg, q, objective["kind"])[0]
     return J
 
 
@@ -348,7 +348,7 @@ def gradient_discrete(S: O.Solver, q0: np.ndarray, steps: int, objective: dict):
         J += cfg.dt * j
         lam = lam + cfg.dt * g
     else:
-        J, lam = O.objective_kinetic_energy(cfg, Q[steps])
+        J, lam = O.terminal_objective(cfg, Q[steps], objective["kind"])
     gf = np.zeros_like(q0)
     for nt in range(steps, 0, -1):
         lam, f = step_vjp(S, Q[nt - 1], lam, nt)

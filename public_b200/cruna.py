@@ -115,6 +115,8 @@ _SIGNATURES = {
     "cruna_profile_enable": (_I, [_P, _I]),
     "cruna_profile_report": (_I, [_P, C.c_char_p, _I]),
     "cruna_set_graphs": (_I, [_P, _I]),
+    "cruna_diagnostics": (_I, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "cruna_diagnostics_dev": (_I, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "cruna_graph_stats": (_I, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "cruna_rhs_direct_noalloc": (_I, [C.POINTER(_Config), _P, _P, _P, C.c_char_p, _I]),
     "cruna_mlp_create": (_I, [_I, C.c_uint64, C.POINTER(_P)]),
@@ -432,9 +434,9 @@ class Cruna:
 
     @staticmethod
     def objective(kind: str, normal: int = 2, index: int = 1, p_inf: float = 0.0) -> Objective:
-        """kind 'plane_p2' (normal, 1-based index, p_inf) or 'kinetic_energy'."""
+        """kind 'plane_p2' (normal, 1-based index, p_inf), 'kinetic_energy' or 'enstrophy' (final time)."""
         o = Objective()
-        o.kind = {"plane_p2": 1, "kinetic_energy": 2}[kind]
+        o.kind = {"plane_p2": 1, "kinetic_energy": 2, "enstrophy": 3}[kind]
         o.normal, o.index, o.p_inf = int(normal), int(index), float(p_inf)
         return o
 
@@ -545,6 +547,18 @@ class Cruna:
         self._check(self.lib.cruna_run_adjoint_dev(self.h, C.c_void_p(qs_ptr), C.c_void_p(Q_ptr),
                                                    None if g_ptr is None else C.c_void_p(g_ptr),
                                                    int(nt_end), int(nsteps)))
+
+    def diagnostics(self, q) -> Tuple[float, float]:
+        """(kinetic energy, enstrophy) volume integrals of a host state."""
+        a = self._state(q)
+        ke, en = C.c_double(), C.c_double()
+        self._check(self.lib.cruna_diagnostics(self.h, _ptr(a), C.byref(ke), C.byref(en)))
+        return ke.value, en.value
+
+    def diagnostics_dev(self, q_ptr: int) -> Tuple[float, float]:
+        ke, en = C.c_double(), C.c_double()
+        self._check(self.lib.cruna_diagnostics_dev(self.h, C.c_void_p(q_ptr), C.byref(ke), C.byref(en)))
+        return ke.value, en.value
 
     def set_graphs(self, on: bool = True):
         """Record repeating loop steps as CUDA graphs inside run / gradient calls (default on)."""

@@ -800,6 +800,33 @@ int cruna_bc_rhss(cruna_ctx *c, double *rhss, const double *qs, const double *q)
   });
 }
 
+static int diagnostics_common(cruna_ctx *c, const double *q_dev, double *ke, double *ens) {
+  if (c->halo_fn) fail(c, CRUNA_ERR_UNSUPPORTED, "volume diagnostics over z slabs are not provided");
+  if (!c->diag) c->diag = dalloc(c, 600);
+  diagnostics_impl(c, q_dev, c->diag + 592, c->diag);
+  double h[2] = {0.0, 0.0};
+  CRUNA_CUDA_CHECK(cudaMemcpyAsync(h, c->diag + 592, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  if (ke) *ke = h[0];
+  if (ens) *ens = h[1];
+  return CRUNA_OK;
+}
+
+// kinetic energy and enstrophy (the volume integrals a case's post-processing forms from snapshots)
+int cruna_diagnostics_dev(cruna_ctx *c, const double *q, double *ke, double *ens) {
+  return guarded(c, [&]() -> int {
+    if (!q) fail(c, CRUNA_ERR_ARG, "null pointer");
+    return diagnostics_common(c, q, ke, ens);
+  });
+}
+
+int cruna_diagnostics(cruna_ctx *c, const double *q, double *ke, double *ens) {
+  return guarded(c, [&]() -> int {
+    if (!q) fail(c, CRUNA_ERR_ARG, "null pointer");
+    return diagnostics_common(c, stage_in(c, 0, q, 5), ke, ens);
+  });
+}
+
 int cruna_check_state_dev(cruna_ctx *c, const double *q) {
   return guarded(c, [&]() -> int {
     if (!q) fail(c, CRUNA_ERR_ARG, "null pointer");
@@ -951,7 +978,8 @@ static int gradient_common(cruna_ctx *c, const double *q0_dev, int nsteps, int n
                            double *J, double *gf_dev, double *gq_dev, int64_t *direct_steps) {
   if (!q0_dev || !obj || !J || nsteps < 1 || nsnap < 1) fail(c, CRUNA_ERR_ARG, "bad arguments to cruna_gradient");
   if (c->halo_fn) fail(c, CRUNA_ERR_UNSUPPORTED, "objective reductions over z slabs are not provided");
-  if (obj->kind != CRUNA_OBJ_PLANE_P2 && obj->kind != CRUNA_OBJ_KINETIC_ENERGY)
+  if (obj->kind != CRUNA_OBJ_PLANE_P2 && obj->kind != CRUNA_OBJ_KINETIC_ENERGY &&
+      obj->kind != CRUNA_OBJ_ENSTROPHY)
     fail(c, CRUNA_ERR_ARG, "unknown objective kind");
   if (obj->kind == CRUNA_OBJ_PLANE_P2) {
     if (obj->normal < 1 || obj->normal > 3) fail(c, CRUNA_ERR_ARG, "objective plane normal must be 1..3");
@@ -991,7 +1019,8 @@ static int optimize_common(cruna_ctx *c, const double *q0, const cruna_objective
   if (obj->kind == CRUNA_OBJ_PLANE_P2 &&
       (obj->normal < 1 || obj->normal > 3 || obj->index < 1 || obj->index > c->cfg.n[obj->normal - 1]))
     fail(c, CRUNA_ERR_ARG, "bad objective plane");
-  if (obj->kind != CRUNA_OBJ_PLANE_P2 && obj->kind != CRUNA_OBJ_KINETIC_ENERGY)
+  if (obj->kind != CRUNA_OBJ_PLANE_P2 && obj->kind != CRUNA_OBJ_KINETIC_ENERGY &&
+      obj->kind != CRUNA_OBJ_ENSTROPHY)
     fail(c, CRUNA_ERR_ARG, "unknown objective kind");
   std::vector<void *> scratch;
   double *saved_user = c->closure_mlp ? c->user_force : c->force;
@@ -1110,7 +1139,8 @@ int cruna_objective_value_dev(cruna_ctx *c, const double *q0, int nsteps, const 
     if (obj->kind == CRUNA_OBJ_PLANE_P2 &&
         (obj->normal < 1 || obj->normal > 3 || obj->index < 1 || obj->index > c->cfg.n[obj->normal - 1]))
       fail(c, CRUNA_ERR_ARG, "bad objective plane");
-    if (obj->kind != CRUNA_OBJ_PLANE_P2 && obj->kind != CRUNA_OBJ_KINETIC_ENERGY)
+    if (obj->kind != CRUNA_OBJ_PLANE_P2 && obj->kind != CRUNA_OBJ_KINETIC_ENERGY &&
+      obj->kind != CRUNA_OBJ_ENSTROPHY)
       fail(c, CRUNA_ERR_ARG, "unknown objective kind");
     std::vector<void *> sc;
     try {

@@ -153,6 +153,7 @@ struct cruna_ctx {
   cruna::HostFactors dhf[3], fhf[3];
   bool vjp_ready = false;
   cruna::LineOpT dopT[3], fopT[3];
+  bool dopT_built[3] = {false, false, false};  // transposed derivative operators (also for objectives)
   double *vjp_ws = nullptr;        // backward workspace (fields)
   double *vjp_st[12] = {nullptr};  // state-sized buffers of the transposed step
   std::vector<double *> vjp_save;  // per boundary row: box values before the row (q, aim / rhs)
@@ -168,6 +169,8 @@ struct cruna_ctx {
   double *cl_force = nullptr;      // forcing + closure stress divergence (5N)
   double *cl_tau = nullptr;        // model stresses (6N) and their derivatives (9N)
   float *cl_x = nullptr, *cl_y = nullptr;  // features (12N) and outputs (6N), point-major
+  double *ens_ws = nullptr;        // enstrophy objective / diagnostics workspace (8N)
+  double *diag = nullptr;          // diagnostics reduction scratch (partials + 2 results)
   // step graphs (step_graph.cu): the cache of the current run call, or null outside one
   bool graphs_enabled = true;
   cruna::StepGraphs *graphs = nullptr;
@@ -206,6 +209,11 @@ void rk_stage(cruna_ctx *c, int stage, double dt, const double *k, const double 
               double *qnext);
 void copy_state(cruna_ctx *c, double *dst, const double *src, int nfields);
 int check_state(cruna_ctx *c, const double *q);
+// out = D_d^T in (one field) with grid spacing h, building the transposed operator on first use
+// (discrete_adjoint.cu); scratch: one field
+void diff_transpose(cruna_ctx *c, int d, const double *in, double *out, double h, double *scratch);
+// kinetic energy and enstrophy of q into out[0], out[1] on the device (gradient.cu); partial: 592 doubles
+void diagnostics_impl(cruna_ctx *c, const double *q, double *out, double *partial);
 
 // step graphs (step_graph.cu): a GraphScope makes a graph cache live for one run call (an inner scope
 // uses the outer one's); graph_step runs body() as the loop step keyed by (kind, a, b, d): eagerly at

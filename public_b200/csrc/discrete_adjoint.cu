@@ -560,7 +560,8 @@ void ensure_vjp(cruna_ctx *c) {
     if (r.type >= 202 && r.type <= 206 && r.type != 204)
       throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint does not transpose the zonal BC types 202/203/205/206"};
   for (int d = 0; d < 3; ++d) {
-    build_transpose(c, c->dop[d], c->dhf[d], c->dopT[d]);
+    if (!c->dopT_built[d]) build_transpose(c, c->dop[d], c->dhf[d], c->dopT[d]);
+    c->dopT_built[d] = true;
     build_transpose(c, c->fop[d], c->fhf[d], c->fopT[d]);
   }
   c->vjp_ws = dalloc(c, (size_t)c->g.N * kVjpFields);
@@ -643,6 +644,14 @@ void step_direct_vjp(cruna_ctx *c, const double *q0, const double *lam1, double 
   lin2(c, dt / 6.0, l1, dth, mu, lk);
   rhs_direct_vjp(c, q0, lk, mu, gf_acc);
   add_fields(c, lam0, mu, c->g.N * 5);
+}
+
+void diff_transpose(cruna_ctx *c, int d, const double *in, double *out, double h, double *scratch) {
+  if (!c->dopT_built[d]) {
+    build_transpose(c, c->dop[d], c->dhf[d], c->dopT[d]);
+    c->dopT_built[d] = true;
+  }
+  apply_T(c, c->dopT[d], d, in, out, diff_scale(c, d, h), 1, 0, scratch);
 }
 
 }  // namespace cruna

@@ -16,6 +16,7 @@
 //                    g = -dj/dq = (0,0,0,0, -2 w (p - p_inf)) on the plane (calc_objective_g; the sign makes
 //                    the backward-integrated qs an approximation of dJ/dq)
 //   kinetic_energy:  J = sum dV |rho u|^2 / (2 rho) at t_T, qs(T) = dJ/dq(T)
+//   enstrophy:       J = sum dV |curl u|^2 / 2 at t_T (the solver's derivative operators), qs(T) = dJ/dq(T)
 // Gradients (calc_grad, force.f90:41-45): dJ/df for a time-constant forcing added to the RHS is the
 // time integral of qs (trapezoid over the adjoint trajectory), dJ/dq0 = qs(0).
 // Discrete mode (cruna_set_adjoint_mode 1) replaces the reference's continuous adjoint step by the
@@ -142,7 +143,118 @@ __global__ void k_axpy(long long M, double a, const double *x, double *y, int ov
     y[p] = overwrite ? a * x[p] : y[p] + a * x[p];
 }
 
+// u_i = (rho u_i) / rho, three fields
+__global__ void k_velocity(long long N, const double *__restrict__ q, double *__restrict__ u) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
+    const double r = q[p];
+    u[p] = q[p + N] / r;
+    u[p + N] = q[p + 2 * N] / r;
+    u[p + 2 * N] = q[p + 3 * N] / r;
+  }
+}
+
+// a = a - b (one field)
+__global__ void k_sub(long long N, double *__restrict__ a, const double *__restrict__ b) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x)
+    a[p] = a[p] - b[p];
+}
+
+// partial sums of dV * 0.5 |omega|^2 (fixed grid and block: deterministic)
+__global__ void k_ens_obj(Grid g, double dV, const double *w, double *partial) {
+  __shared__ double sh[RB];
+  double acc = 0.0;
+  const long long N = g.N;
+  for (long long p = blockIdx.x * (long long)RB + threadIdx.x; p < N; p += (long long)RG * RB) {
+    const double a = w[p], b = w[p + N], d = w[p + 2 * N];
+    acc += dV * 0.5 * (a * a + b * b + d * d);
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = RB / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+// lam(1..3) hold curl^T omega on entry; dZ/dq = (-sum u_i gu_i / rho, gu_i / rho, 0), gu = dV curl^T omega
+__global__ void k_ens_grad(long long N, double dV, const double *__restrict__ q, const double *__restrict__ u,
+                           double *__restrict__ lam) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
+    const double r = q[p];
+    const double g1 = dV * lam[p + N], g2 = dV * lam[p + 2 * N], g3 = dV * lam[p + 3 * N];
+    lam[p] = -(u[p] * g1 + u[p + N] * g2 + u[p + 2 * N] * g3) / r;
+    lam[p + N] = g1 / r;
+    lam[p + 2 * N] = g2 / r;
+    lam[p + 3 * N] = g3 / r;
+    lam[p + 4 * N] = 0.0;
+  }
+}
+
 }  // namespace
+
+double cell_volume(const cruna_ctx *c) {
+  double dV = 1.0;
+  for (int d = 0; d < 3; ++d)
+    if (c->cfg.n[d] > 1) dV *= c->dx[d];
+  return dV;
+}
+
+// Z = sum dV |curl u|^2 / 2 with the context's derivative operators (h = dx) into J (scaled by 1,
+// accumulated or not); lam (optional) = dZ/dq through the transposed operators.  Workspace: 8 fields.
+void enstrophy_objective(cruna_ctx *c, const double *q, double *lam, double *partial, double *J, int accumulate) {
+  const long long N = c->g.N;
+  if (!c->ens_ws) c->ens_ws = dalloc(c, (size_t)N * 8);
+  double *u = c->ens_ws, *w = u + 3 * N, *t = u + 6 * N, *scr = u + 7 * N;
+  const int blocks = (int)std::min<long long>((N + 255) / 256, 148LL * 16);
+  k_velocity<<<blocks, 256, 0, c->stream>>>(N, q, u);
+  CRUNA_LAUNCH_CHECK(c);
+  const double *dx = c->dx;
+  auto D = [&](int d, const double *f, double *out) { apply_diff(c, d, f, nullptr, out, dx[d], 1); };
+  auto sub = [&](double *a, const double *b) {
+    k_sub<<<blocks, 256, 0, c->stream>>>(N, a, b);
+    CRUNA_LAUNCH_CHECK(c);
+  };
+  double *wx = w, *wy = w + N, *wz = w + 2 * N;
+  const double *u1 = u, *u2 = u + N, *u3 = u + 2 * N;
+  D(1, u3, wx); D(2, u2, t); sub(wx, t);   // D_y w - D_z v
+  D(2, u1, wy); D(0, u3, t); sub(wy, t);   // D_z u - D_x w
+  D(0, u2, wz); D(1, u1, t); sub(wz, t);   // D_x v - D_y u
+  k_ens_obj<<<RG, RB, 0, c->stream>>>(c->g, cell_volume(c), w, partial);
+  CRUNA_LAUNCH_CHECK(c);
+  k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, 1.0, accumulate);
+  CRUNA_LAUNCH_CHECK(c);
+  if (!lam) return;
+  auto DT = [&](int d, const double *f, double *out) { diff_transpose(c, d, f, out, dx[d], scr); };
+  double *g1 = lam + N, *g2 = lam + 2 * N, *g3 = lam + 3 * N;
+  DT(2, wy, g1); DT(1, wz, t); sub(g1, t);   // D_z^T omega_y - D_y^T omega_z
+  DT(0, wz, g2); DT(2, wx, t); sub(g2, t);   // D_x^T omega_z - D_z^T omega_x
+  DT(1, wx, g3); DT(0, wy, t); sub(g3, t);   // D_y^T omega_x - D_x^T omega_y
+  k_ens_grad<<<blocks, 256, 0, c->stream>>>(N, cell_volume(c), q, u, lam);
+  CRUNA_LAUNCH_CHECK(c);
+}
+
+// the final-time objectives: J (overwritten) and, with lam, lam = dJ/dq
+void terminal_objective(cruna_ctx *c, const cruna_objective *obj, const double *q, double *lam, double *partial,
+                        double *J) {
+  if (obj->kind == CRUNA_OBJ_ENSTROPHY) {
+    enstrophy_objective(c, q, lam, partial, J, 0);
+    return;
+  }
+  k_ke_obj<<<RG, RB, 0, c->stream>>>(c->g, cell_volume(c), q, lam, partial);
+  CRUNA_LAUNCH_CHECK(c);
+  k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, 1.0, 0);
+  CRUNA_LAUNCH_CHECK(c);
+}
+
+// kinetic energy and enstrophy of a state into out[0], out[1] (device)
+void diagnostics_impl(cruna_ctx *c, const double *q, double *out, double *partial) {
+  k_ke_obj<<<RG, RB, 0, c->stream>>>(c->g, cell_volume(c), q, nullptr, partial);
+  CRUNA_LAUNCH_CHECK(c);
+  k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, out, 1.0, 0);
+  CRUNA_LAUNCH_CHECK(c);
+  enstrophy_objective(c, q, nullptr, partial, out + 1, 0);
+}
 
 struct GradientRun {
   cruna_ctx *c;
@@ -209,13 +321,7 @@ struct GradientRun {
         plane_source(qN);
         axpy(dt, gsrc, qs, true);
       } else {
-        double dV = 1.0;
-        for (int d = 0; d < 3; ++d)
-          if (c->cfg.n[d] > 1) dV *= c->dx[d];
-        k_ke_obj<<<RG, RB, 0, c->stream>>>(c->g, dV, qN, qs, partial);
-        CRUNA_LAUNCH_CHECK(c);
-        k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, 1.0, 0);
-        CRUNA_LAUNCH_CHECK(c);
+        terminal_objective(c, obj, qN, qs, partial, J);
       }
     }
     step_direct_vjp(c, qnt, qs, qs, gf, nt + 1);
@@ -233,15 +339,7 @@ struct GradientRun {
     const double dt = c->cfg.dt;
     const bool plane = obj->kind == CRUNA_OBJ_PLANE_P2;
     if (nt == nsteps) {
-      if (obj->kind == CRUNA_OBJ_KINETIC_ENERGY) {
-        double dV = 1.0;
-        for (int d = 0; d < 3; ++d)
-          if (c->cfg.n[d] > 1) dV *= c->dx[d];
-        k_ke_obj<<<RG, RB, 0, c->stream>>>(c->g, dV, qnt, qs, partial);
-        CRUNA_LAUNCH_CHECK(c);
-        k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, 1.0, 0);
-        CRUNA_LAUNCH_CHECK(c);
-      }
+      if (!plane) terminal_objective(c, obj, qnt, qs, partial, J);
       if (gf) axpy(0.5 * dt, qs, gf, true);
     }
     if (plane) {
@@ -354,11 +452,9 @@ double objective_direct_impl(cruna_ctx *c, const double *q0, int nsteps, const c
   copy_state(c, work, q0, 5);
   const bool plane = obj->kind == CRUNA_OBJ_PLANE_P2;
   const int nd = obj->normal - 1;
-  double w = 1.0, dV = 1.0;
-  for (int d = 0; d < 3; ++d) {
-    if (c->cfg.n[d] > 1) dV *= c->dx[d];
+  double w = 1.0;
+  for (int d = 0; d < 3; ++d)
     if (d != nd && c->cfg.n[d] > 1) w *= c->dx[d];
-  }
   for (int nt = 1; nt <= nsteps; ++nt) {
     direct_loop_step(c, work, nt);
     if (plane) {
@@ -368,12 +464,7 @@ double objective_direct_impl(cruna_ctx *c, const double *q0, int nsteps, const c
       CRUNA_LAUNCH_CHECK(c);
     }
   }
-  if (!plane) {
-    k_ke_obj<<<RG, RB, 0, c->stream>>>(c->g, dV, work, nullptr, partial);
-    CRUNA_LAUNCH_CHECK(c);
-    k_sum_partials<<<1, 32, 0, c->stream>>>(partial, RG, J, 1.0, 0);
-    CRUNA_LAUNCH_CHECK(c);
-  }
+  if (!plane) terminal_objective(c, obj, work, nullptr, partial, J);
   double h = 0.0;
   CRUNA_CUDA_CHECK(cudaMemcpyAsync(&h, J, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));

@@ -51,6 +51,8 @@ def run(args) -> dict:
         d = np.zeros((N, 5))
         d[:, 4] = rng.standard_normal(N)
         dirs.append(torch.from_numpy(np.ascontiguousarray(d.T.ravel())).to(dev))
+    # the library's _dev calls run on its own stream: every torch result they read must be complete
+    torch.cuda.synchronize()
     with Cruna(Settings.from_dict(s), qref=q0, force=np.zeros_like(q0)) as c:
         obj = c.objective("plane_p2", normal=2, index=j_plane, p_inf=p_inf)
         c.set_forcing_dev(f.data_ptr())
@@ -62,9 +64,11 @@ def run(args) -> dict:
             vals = []
             for d in dirs:
                 fp = f + eps * d
+                torch.cuda.current_stream().synchronize()
                 c.set_forcing_dev(fp.data_ptr())
                 Jp = c.objective_value_dev(q.data_ptr(), args.steps, obj)
                 fm = f - eps * d
+                torch.cuda.current_stream().synchronize()
                 c.set_forcing_dev(fm.data_ptr())
                 Jm = c.objective_value_dev(q.data_ptr(), args.steps, obj)
                 vals.append((Jp - Jm) / (2 * eps))

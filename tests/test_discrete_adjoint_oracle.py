@@ -153,3 +153,29 @@ def test_optimisation_loop_reduces_the_objective():
                                     discrete=discrete)
         assert Js[1] < 0.5 * Js[0] and Js[2] <= Js[1] * 1.001, (discrete, Js)
         assert np.all(alphas > 0)
+
+
+@pytest.mark.parametrize("scheme", ["o8_e_c_p", "o6_i_c_p"])
+def test_enstrophy_gradient_matches_finite_differences(scheme):
+    """dZ/dq of the enstrophy objective (curl with the solver's operators, transposed for the gradient)."""
+    s, q = cases.taylor_green(n=10, seed=1)
+    s["diff"] = (scheme,) * 3
+    cfg = ocfg(s)
+    Z, g = O.objective_enstrophy(cfg, q)
+    rng = np.random.default_rng(0)
+    d = rng.standard_normal(q.shape)
+    eps = 1e-6
+    fd = (O.objective_enstrophy(cfg, q + eps * d)[0] - O.objective_enstrophy(cfg, q - eps * d)[0]) / (2 * eps)
+    assert Z > 0 and abs(fd - np.sum(g * d)) < 1e-8 * abs(fd)
+
+
+def test_enstrophy_gradient_through_steps():
+    s, q = cases.taylor_green(n=12, seed=0)
+    s["mu0"] = 0.02
+    S = O.Solver(ocfg(s), force=np.zeros_like(q))
+    eq, ef = grad_mismatch(S, q, 3, {"kind": "enstrophy"}, eps=1e-6)
+    assert eq < 1e-7 and ef < 1e-6, (eq, ef)
+    _, gfd, gqd = DA.gradient_discrete(S, q, 3, {"kind": "enstrophy"})
+    _, gfc, gqc = O.gradient_store_all(S, q, 3, {"kind": "enstrophy"})
+    cos = float(np.sum(gqc * gqd) / np.linalg.norm(gqc) / np.linalg.norm(gqd))
+    assert cos > 0.9999, cos

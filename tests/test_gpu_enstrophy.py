@@ -1,0 +1,78 @@
+"""Enstrophy: the volume diagnostics (kinetic energy, enstrophy) and the final-time enstrophy
+objective's gradients (continuous and exact discrete adjoint) through the C ABI against the oracle
+(oracle/cruna_oracle.py: objective_enstrophy, gradient_store_all; oracle/discrete_adjoint.py:
+gradient_discrete).  Tolerances: diagnostics 1e-12 relative; J 1e-12 relative; gradients 1e-10
+relative L2 per variable (measured against max(its norm, 1e-3 of the state's norm))."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import cruna_oracle as O
+from oracle import discrete_adjoint as DA
+from public_b200 import cases
+from public_b200.cruna import Cruna, Settings
+
+pytestmark = pytest.mark.gpu
+CFG_FIELDS = {f.name for f in O.dataclasses.fields(O.Config)}
+
+
+def ocfg(s):
+    return O.Config(**{k: v for k, v in s.items() if k in CFG_FIELDS})
+
+
+def cot_err(a, b):
+    scale = np.linalg.norm(b.ravel())
+    return max(float(np.linalg.norm((a[..., v] - b[..., v]).ravel()) /
+                     max(np.linalg.norm(b[..., v].ravel()), 1e-3 * scale)) for v in range(b.shape[-1]))
+
+
+@pytest.mark.parametrize("case", ["tgv", "tgv_compact", "mixing", "vortex"])
+def test_diagnostics_match_oracle(case):
+    if case == "mixing":
+        s, q = cases.mixing_layer(n=(24, 22, 12))
+    elif case == "vortex":
+        s, q = cases.isentropic_vortex(n=32)
+    else:
+        s, q = cases.taylor_green(n=16, seed=2)
+        if case == "tgv_compact":
+            s["diff"] = ("o6_i_c_p",) * 3
+    cfg = ocfg(s)
+    ke_ref = O.objective_kinetic_energy(cfg, q)[0]
+    z_ref = O.objective_enstrophy(cfg, q)[0]
+    with Cruna(Settings.from_dict(s), qref=q) as c:
+        ke, z = c.diagnostics(q)
+        qt = torch.from_numpy(np.ascontiguousarray(q.ravel(order="F"))).cuda()
+        assert c.diagnostics_dev(qt.data_ptr()) == (ke, z)
+    assert abs(ke - ke_ref) < 1e-12 * abs(ke_ref)
+    assert abs(z - z_ref) < 1e-12 * abs(z_ref), (z, z_ref)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_enstrophy_gradient_matches_oracle(mode):
+    s, q = cases.taylor_green(n=12, seed=0)
+    s["mu0"] = 0.02
+    S = O.Solver(ocfg(s), force=np.zeros_like(q))
+    obj = {"kind": "enstrophy"}
+    if mode == 0:
+        J_ref, gf_ref, gq_ref = O.gradient_store_all(S, q, 4, obj)
+    else:
+        J_ref, gf_ref, gq_ref = DA.gradient_discrete(S, q, 4, obj)
+    with Cruna(Settings.from_dict(s), force=np.zeros_like(q)) as c:
+        c.set_adjoint_mode(mode)
+        J, gf, gq, steps = c.gradient(q, 4, 2, c.objective("enstrophy"))
+        Jv = c.objective_value(q, 4, c.objective("enstrophy"))
+    assert abs(J - J_ref) < 1e-12 * abs(J_ref) and abs(Jv - J_ref) < 1e-12 * abs(J_ref)
+    assert cot_err(gq, gq_ref) < 1e-10, cot_err(gq, gq_ref)
+    assert cot_err(gf, gf_ref) < 1e-10, cot_err(gf, gf_ref)
+
+
+def test_enstrophy_gradient_fp32_stencils_close_to_fp64():
+    s, q = cases.taylor_green(n=16, seed=0)
+    s["mu0"] = 0.02
+    out = {}
+    for prec in ("fp64", "fp32"):
+        with Cruna(Settings.from_dict(dict(s, precision=prec)), force=np.zeros_like(q)) as c:
+            out[prec] = c.gradient(q, 6, 3, c.objective("enstrophy"))
+    (J64, gf64, gq64, _), (J32, gf32, gq32, _) = out["fp64"], out["fp32"]
+    assert abs(J32 - J64) < 1e-6 * abs(J64)
+    assert np.linalg.norm(gq32 - gq64) < 1e-5 * np.linalg.norm(gq64)
