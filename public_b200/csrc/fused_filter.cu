@@ -3,11 +3,10 @@
 // counterpart: the interior stencil of filter_pen_core_o10_i_c_o.f90:182-199 at alpha = 0 with
 // periodic wrap, blended q <- q - s*(q - F q)).
 //
-// With all three directions due, one z-marching pass applies them in the reference's order (x, y
-// on staged plane tiles, z from a per-thread queue of 11 filtered planes) and reads and writes the
-// state once.  Otherwise two passes: pass 1 filters each plane in x and then y on 32 x 32 tiles with
-// 5-wide halos (corners included, so the y filter sees x-filtered halo rows); pass 2 filters in z
-// with a per-thread register queue of 11 planes.
+// Two passes apply the three directional filters in the reference's order to all five variables:
+// pass 1 filters each plane in x and then y on 32 x 32 tiles with 5-wide halos (corners included,
+// so the y filter sees x-filtered halo rows); pass 2 filters in z with a per-thread register queue
+// of 11 planes.  Each pass reads and writes the state once.
 #include "cruna_internal.cuh"
 #include "fused_common.cuh"
 
@@ -40,7 +39,7 @@ __device__ __forceinline__ double filt(const FilterArgs &a, const double *p, int
 }
 
 // pass 1: x then y filter of one plane, one variable at a time (tile offsets computed once)
-__global__ void __launch_bounds__(FTHR) k_filter_xy(const __grid_constant__ FilterArgs a) {
+__global__ void __launch_bounds__(FTHR, 4) k_filter_xy(const __grid_constant__ FilterArgs a) {
   constexpr int PW = FXT + 2 * FR, PH = FYT + 2 * FR;
   constexpr int NL = (PW * PH + FTHR - 1) / FTHR;
   __shared__ double raw[PH * PW];
@@ -129,87 +128,6 @@ __global__ void __launch_bounds__(FTHR) k_filter_z(const __grid_constant__ Filte
   }
 }
 
-// x, y and z filters in one pass: a block owns one variable on a 32 x 16 tile of the x-y plane and
-// marches z over its chunk plus FR planes either side.  Per plane it stages the tile with its x-y
-// halos in shared memory, filters in x, then in y (two rows per thread from a register window), and
-// pushes the result into a per-thread queue of 2*FR+1 planes; the z filter of the plane FR behind is
-// then written out.  The next plane's tile is loaded one plane ahead.  Same arithmetic and order as
-// k_filter_xy followed by k_filter_z; the state is read once and written once.
-constexpr int GXT = 32, GYT = 16, GTHR = 256, GRPT = GYT / (GTHR / GXT);
-
-__global__ void __launch_bounds__(GTHR, 3) k_filter_xyz(const __grid_constant__ FilterArgs a) {
-  constexpr int PW = GXT + 2 * FR, PH = GYT + 2 * FR;
-  constexpr int NL = (PW * PH + GTHR - 1) / GTHR;
-  constexpr int NQ = 2 * FR + 1, NW = GRPT + 2 * FR;
-  __shared__ double raw[PH * PW];
-  __shared__ double xf[PH * GXT];
-  const int tid = threadIdx.x;
-  const int i0 = blockIdx.x * GXT, j0 = blockIdx.y * GYT;
-  const int v = blockIdx.z % 5, chunk = blockIdx.z / 5;
-  const int n3 = a.n[2];
-  const int k0 = chunk * a.kc, k1 = min(k0 + a.kc, a.g.n3);
-  const long long N = a.g.N, n1 = a.g.n1, n12 = (long long)a.g.n1 * a.g.n2;
-  const double *in = a.in + v * N;
-  double *out = a.out + v * N;
-  int goff[NL];
-#pragma unroll
-  for (int m = 0; m < NL; ++m) {
-    const int c = tid + m * GTHR;
-    goff[m] = -1;
-    if (c < PW * PH) {
-      const int lx = c % PW - FR, ly = c / PW - FR;
-      const int gi = a.on[0] ? wrapi(i0 + lx, a.n[0]) : min(max(i0 + lx, 0), a.n[0] - 1);
-      const int gj = a.on[1] ? wrapi(j0 + ly, a.n[1]) : min(max(j0 + ly, 0), a.n[1] - 1);
-      goff[m] = gi + (int)n1 * gj;
-    }
-  }
-  const int lx = tid % GXT, ly0 = (tid / GXT) * GRPT;
-  const int gi = i0 + lx;
-  double q[GRPT][NQ];
-  double nxt[NL];
-  {
-    const long long kofs = n12 * wrapi(k0 - FR, n3);
-#pragma unroll
-    for (int m = 0; m < NL; ++m)
-      if (goff[m] >= 0) nxt[m] = in[goff[m] + kofs];
-  }
-  for (int kk = k0 - FR; kk < k1 + FR; ++kk) {
-#pragma unroll
-    for (int m = 0; m < NL; ++m)
-      if (goff[m] >= 0) raw[tid + m * GTHR] = nxt[m];
-    if (kk + 1 < k1 + FR) {
-      const long long kofs = n12 * wrapi(kk + 1, n3);
-#pragma unroll
-      for (int m = 0; m < NL; ++m)
-        if (goff[m] >= 0) nxt[m] = in[goff[m] + kofs];
-    }
-    __syncthreads();
-    for (int c = tid; c < GXT * PH; c += GTHR) {
-      const int cx = c % GXT, cy = c / GXT;
-      const double *p = raw + cy * PW + cx + FR;
-      xf[c] = a.on[0] ? filt(a, p, 1) : p[0];
-    }
-    __syncthreads();
-    double w[NW];
-#pragma unroll
-    for (int m = 0; m < NW; ++m) w[m] = xf[(ly0 + m) * GXT + lx];
-#pragma unroll
-    for (int r = 0; r < GRPT; ++r) {
-#pragma unroll
-      for (int m = 0; m < NQ - 1; ++m) q[r][m] = q[r][m + 1];
-      q[r][NQ - 1] = a.on[1] ? filt(a, w + r + FR, 1) : w[r + FR];
-    }
-    if (kk >= k0 + FR && gi < a.g.n1) {  // the queue holds planes kk - 2FR .. kk: filter kk - FR in z
-      const long long kofs = n12 * (kk - FR);
-#pragma unroll
-      for (int r = 0; r < GRPT; ++r) {
-        const int gj = j0 + ly0 + r;
-        if (gj < a.g.n2) out[gi + n1 * gj + kofs] = filt(a, q[r] + FR, 1);
-      }
-    }
-  }
-}
-
 }  // namespace
 
 // filters usable by the fused passes: the explicit periodic o10 filter or none, in every direction
@@ -251,20 +169,6 @@ void filter3_fused(cruna_ctx *c, const double *in, double *out, const int on_in[
       for (int m = 0; m <= FR; ++m) a.c[m] = c->fop[d].c[m];
       a.blend = c->fop[d].blend;
     }
-  if (a.on[2] && (a.on[0] || a.on[1]) && c->g.n3 > 2 * FR) {
-    a.in = in;
-    a.out = out;
-    const int bx = (c->g.n1 + GXT - 1) / GXT, by = (c->g.n2 + GYT - 1) / GYT;
-    const int n3 = c->g.n3;
-    // z chunks: enough blocks for about two rounds of resident blocks, each chunk at least 32 planes
-    int nz = std::max(1, std::min(std::max(1, n3 / 32), (6 * 148 + 5 * bx * by - 1) / (5 * bx * by)));
-    a.kc = (n3 + nz - 1) / nz;
-    nz = (n3 + a.kc - 1) / a.kc;
-    ProfScope ps(c, "filter_xyz");
-    k_filter_xyz<<<dim3(bx, by, 5 * nz), GTHR, 0, c->stream>>>(a);
-    CRUNA_LAUNCH_CHECK(c);
-    return;
-  }
   double *tmp = c->st[0];
   const double *src = in;
   a.kc = 1;
