@@ -302,6 +302,12 @@ int cruna_box_filter_dev(cruna_ctx *ctx, int factor, const double *q, double *q_
 /* Closure features of a coarse state (n x 12 floats, point-major): du_i/dx_j with the context's
    derivative scheme, rho, T, delta. */
 int cruna_closure_features_dev(cruna_ctx *ctx, const double *q, double delta, float *X);
+/* Scale-free closure (0 default, 1 on): with g = |grad u| (Frobenius norm of the coarse velocity
+   gradient) at each point, features 0..8 become grad u / g and feature 11 becomes g * delta, and the
+   network's outputs are read as tau_ij / (rho (g delta)^2) and multiplied back.  Affects
+   cruna_closure_features_dev and the closure inside the RHS; a network trained on normalised pairs
+   then carries over while the flow decays. */
+int cruna_set_closure_normalisation(cruna_ctx *ctx, int on);
 /* Attach (mlp != NULL) or detach the closure: every direct RHS evaluation of ctx then adds
    -d_j tau_ij(model) to the momentum equations, on top of the forcing set with cruna_set_forcing.  The
    MLP must outlive the attachment; the discrete adjoint (mode 1) is unavailable while attached. */

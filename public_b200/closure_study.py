@@ -12,7 +12,10 @@
    each run (CUDA events, excluding set-up) with the fine DNS's.
 
     python -m public_b200.closure_study [--n 256] [--factor 4] [--steps 3000] [--every 10]
-        [--samples 2000000] [--train-steps 3000] [--batch 4096] [--lr 1e-3] [--json out.json]
+        [--samples 2000000] [--train-steps 3000] [--batch 4096] [--lr 1e-3] [--normalised] [--json out.json]
+
+--normalised trains and runs the scale-free closure (``cruna_set_closure_normalisation``): features
+grad u / |grad u| and |grad u| delta, targets tau / (rho (|grad u| delta)^2).
 
 Prints one JSON object.  Data are synthetic (seeded spectrum, no dataset).
 """
@@ -65,6 +68,7 @@ def run(args) -> dict:
     Xs, Ys = [], []
     ke_dns, t_dns = [], []
     with Cruna(Settings.from_dict(s)) as fine, Cruna(Settings.from_dict(sc)) as coarse:
+        coarse.set_closure_normalisation(args.normalised)
         # initial filtered state (start of both coarse runs)
         fine.box_filter_dev(r, q.data_ptr(), qc.data_ptr(), tau.data_ptr())
         fine.sync()
@@ -90,21 +94,25 @@ def run(args) -> dict:
             t_dns.append((k + 1) * args.every * dt_f)
         X = torch.cat(Xs).contiguous()
         Y = torch.cat(Ys).contiguous()
+        # normalised closure: targets tau / (rho (g delta)^2), rho and g delta being features 9 and 11
+        scale = (X[:, 9] * X[:, 11] * X[:, 11]).unsqueeze(1) if args.normalised else torch.ones_like(Y[:, :1])
+        scale = torch.where(scale > 0, scale, torch.ones_like(scale))
+        Yt = (Y / scale).contiguous()
         in_mean = X.mean(0).cpu().numpy()
         in_scale = X.std(0).cpu().numpy()
         in_scale[in_scale <= 1e-12] = 1.0     # constant features (the filter width)
-        out_scale = Y.std(0).cpu().numpy()
+        out_scale = Yt.std(0).cpu().numpy()
         out_scale[out_scale <= 1e-30] = 1.0
         nb = (X.shape[0] // args.batch) * args.batch
-        X, Y = X[:nb].contiguous(), Y[:nb].contiguous()
+        X, Y, Yt, scale = X[:nb].contiguous(), Y[:nb].contiguous(), Yt[:nb].contiguous(), scale[:nb]
 
         mlp = ClosureMLP(0, seed=args.seed)
         mlp.set_scaling(in_mean, in_scale, out_scale)
         t0 = time.time()
-        hist = mlp.train(X, Y, batch=args.batch, steps=args.train_steps, lr=args.lr, seed=args.seed)
+        hist = mlp.train(X, Yt, batch=args.batch, steps=args.train_steps, lr=args.lr, seed=args.seed)
         train_s = time.time() - t0
         # explained variance of the stresses on the training pairs
-        pred = mlp.forward(X)
+        pred = mlp.forward(X) * scale
         ev = 1.0 - float(((pred - Y) ** 2).sum().item()) / float(((Y - Y.mean(0)) ** 2).sum().item())
 
         def coarse_run(with_closure: bool):
@@ -135,6 +143,7 @@ def run(args) -> dict:
         "workload": f"isotropic turbulence {nf}^3 -> {nc}^3 (box filter x{r}), Mach_t {args.mach_t}, "
                     f"Re_lambda {args.re_lambda}, {args.steps} fine steps",
         "samples": int(X.shape[0]), "train_steps": args.train_steps, "batch": args.batch,
+        "normalised": bool(args.normalised),
         "train_loss_first": float(hist[0]) if len(hist) else None,
         "train_loss_last": float(np.mean(hist[-20:])) if len(hist) else None,
         "explained_variance": ev, "train_seconds": train_s,
@@ -162,6 +171,8 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--mach-t", type=float, default=0.3)
     ap.add_argument("--re-lambda", type=float, default=100.0)
+    ap.add_argument("--normalised", action="store_true",
+                    help="scale-free closure: features grad u / |grad u|, |grad u| delta; targets tau / (rho (|grad u| delta)^2)")
     ap.add_argument("--json", type=str, default=None)
     args = ap.parse_args(argv)
     out = run(args)

@@ -115,6 +115,7 @@ _SIGNATURES = {
     "cruna_profile_enable": (_I, [_P, _I]),
     "cruna_profile_report": (_I, [_P, C.c_char_p, _I]),
     "cruna_set_graphs": (_I, [_P, _I]),
+    "cruna_set_closure_normalisation": (_I, [_P, _I]),
     "cruna_diagnostics": (_I, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "cruna_diagnostics_dev": (_I, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "cruna_graph_stats": (_I, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
@@ -448,6 +449,10 @@ class Cruna:
 
     def closure_features_dev(self, q_ptr: int, delta: float, x_ptr: int):
         self._check(self.lib.cruna_closure_features_dev(self.h, C.c_void_p(q_ptr), float(delta), C.c_void_p(x_ptr)))
+
+    def set_closure_normalisation(self, on: bool = True):
+        """Scale-free closure features and outputs (grad u / |grad u|, |grad u| delta; tau / (rho (|grad u| delta)^2))."""
+        self._check(self.lib.cruna_set_closure_normalisation(self.h, 1 if on else 0))
 
     def set_closure(self, mlp, delta: float = 0.0):
         """Attach a public_b200.closure.ClosureMLP (None detaches)."""

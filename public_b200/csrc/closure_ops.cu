@@ -7,7 +7,8 @@
 //   tau_ij = mean(rho u_i u_j) - mean(rho u_i) mean(rho u_j) / mean(rho),
 // so the filtered momentum equation reads d(rho u_i)/dt + d_j(rho u_i u_j)_resolved + ... = -d_j tau_ij.
 // Features (12 per point): du_i/dx_j of the coarse velocity (u_x, u_y, u_z, v_x, ..., w_z, derivatives
-// of the solver's own scheme), rho, T, the filter width.  With a closure attached, every direct RHS
+// of the solver's own scheme), rho, T, the filter width; or, normalised, du_i/dx_j / g, rho, T, g delta
+// with g = |grad u| (Frobenius), and the network's outputs scaled by rho (g delta)^2.  With a closure attached, every direct RHS
 // evaluation adds -d_j tau_ij(model) to the momentum equations through the forcing hook (apply_force,
 // src/opt/force.f90:27-31), on top of the caller's own forcing.
 #include <algorithm>
@@ -53,24 +54,36 @@ __global__ void k_box_filter(Grid fg, Grid cg, int r0, int r1, int r2, const dou
   }
 }
 
-// features from the generic workspace (u, T, grad u) and rho
+// features from the generic workspace (u, T, grad u) and rho; normalised: grad u / |grad u| and
+// |grad u| * delta in place of the raw gradients and the filter width
 __global__ void k_features(long long N, const double *__restrict__ q, const double *__restrict__ t, double delta,
-                           float *__restrict__ X) {
+                           int norm, float *__restrict__ X) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
        p += (long long)gridDim.x * blockDim.x) {
     float *x = X + p * 12;
-    for (int g = 0; g < 9; ++g) x[g] = (float)t[p + (long long)(F_UX + g) * N];
+    double gr[9], s = 0.0;
+    for (int g = 0; g < 9; ++g) {
+      gr[g] = t[p + (long long)(F_UX + g) * N];
+      s += gr[g] * gr[g];
+    }
+    const double gm = sqrt(s), inv = gm > 0.0 ? 1.0 / gm : 0.0;
+    for (int g = 0; g < 9; ++g) x[g] = (float)(norm ? gr[g] * inv : gr[g]);
     x[9] = (float)q[p];
     x[10] = (float)t[p + (long long)F_T * N];
-    x[11] = (float)delta;
+    x[11] = (float)(norm ? gm * delta : delta);
   }
 }
 
-// model stresses (point-major floats) -> six double fields tau_11, tau_22, tau_33, tau_12, tau_13, tau_23
-__global__ void k_tau_fields(long long N, const float *__restrict__ Y, double *__restrict__ tau) {
+// model stresses (point-major floats) -> six double fields tau_11, tau_22, tau_33, tau_12, tau_13, tau_23;
+// normalised outputs are tau / (rho (|grad u| delta)^2), rho and |grad u| delta read back from the features
+__global__ void k_tau_fields(long long N, const float *__restrict__ Y, const float *__restrict__ X, int norm,
+                             double *__restrict__ tau) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N;
-       p += (long long)gridDim.x * blockDim.x)
-    for (int t = 0; t < 6; ++t) tau[p + t * N] = (double)Y[p * 6 + t];
+       p += (long long)gridDim.x * blockDim.x) {
+    const double gd = (double)X[p * 12 + 11];
+    const double sc = norm ? (double)X[p * 12 + 9] * gd * gd : 1.0;
+    for (int t = 0; t < 6; ++t) tau[p + t * N] = (double)Y[p * 6 + t] * sc;
+  }
 }
 
 // f = user forcing (or 0) with f_{1+i} -= sum_j d_j tau_ij; dtau[i*3 + j] = d_j tau_ij
@@ -97,7 +110,8 @@ void features(cruna_ctx *c, const double *q, double delta, float *X) {
   ensure_generic(c);
   generic_forward_gradients(c, q);
   const long long N = c->g.N;
-  k_features<<<(int)std::min<long long>(nblocks(N), 148LL * 32), kThreads, 0, c->stream>>>(N, q, c->tmp, delta, X);
+  k_features<<<(int)std::min<long long>(nblocks(N), 148LL * 32), kThreads, 0, c->stream>>>(
+      N, q, c->tmp, delta, c->closure_norm ? 1 : 0, X);
   CRUNA_LAUNCH_CHECK(c);
 }
 
@@ -117,7 +131,7 @@ void closure_stage(cruna_ctx *c, const double *q) {
   features(c, q, c->closure_delta, c->cl_x);
   mlp_forward_stream(c->closure_mlp, c->cl_x, c->cl_y, N, c->stream);
   const int blocks = (int)std::min<long long>(nblocks(N), 148LL * 32);
-  k_tau_fields<<<blocks, kThreads, 0, c->stream>>>(N, c->cl_y, c->cl_tau);
+  k_tau_fields<<<blocks, kThreads, 0, c->stream>>>(N, c->cl_y, c->cl_x, c->closure_norm ? 1 : 0, c->cl_tau);
   CRUNA_LAUNCH_CHECK(c);
   double *dtau = c->cl_tau + 6 * N;
   for (int i = 0; i < 3; ++i)
@@ -177,6 +191,13 @@ int cruna_closure_features_dev(cruna_ctx *c, const double *q, double delta, floa
   return closure_guard(c, [&]() -> int {
     if (!q || !X) throw ApiError{CRUNA_ERR_ARG, "null pointer"};
     features(c, q, delta, X);
+    return CRUNA_OK;
+  });
+}
+
+int cruna_set_closure_normalisation(cruna_ctx *c, int on) {
+  return closure_guard(c, [&]() -> int {
+    c->closure_norm = on != 0;
     return CRUNA_OK;
   });
 }

@@ -165,6 +165,7 @@ struct cruna_ctx {
   // learned subgrid closure (closure_ops.cu): active when mlp is set
   struct cruna_mlp *closure_mlp = nullptr;
   double closure_delta = 0.0;
+  bool closure_norm = false;       // scale-free features / outputs (cruna_set_closure_normalisation)
   double *user_force = nullptr;    // the caller's forcing (cruna_set_forcing) while a closure is set
   double *cl_force = nullptr;      // forcing + closure stress divergence (5N)
   double *cl_tau = nullptr;        // model stresses (6N) and their derivatives (9N)

@@ -102,12 +102,13 @@ def test_closure_adds_model_stress_divergence():
     assert np.max(np.abs(back - no_f + (with_cl - plain))) < 1e-9 * np.max(np.abs(plain))
 
 
-def test_small_closure_study_runs_end_to_end():
+@pytest.mark.parametrize("normalised", [False, True])
+def test_small_closure_study_runs_end_to_end(normalised):
     from public_b200 import closure_study
     import argparse
     args = argparse.Namespace(
         n=64, factor=4, steps=40, every=10, samples=8192, train_steps=60, batch=512, lr=2e-3, seed=3,
-        mach_t=0.3, re_lambda=60.0, json=None)
+        mach_t=0.3, re_lambda=60.0, normalised=normalised, json=None)
     out = closure_study.run(args)
     assert out["samples"] >= 512
     assert out["train_loss_last"] < out["train_loss_first"]
@@ -115,3 +116,41 @@ def test_small_closure_study_runs_end_to_end():
         assert len(out[key]) == 5 and all(np.isfinite(out[key]))
     assert out["ke_decay_dns"] < 1.0
     assert out["ke_max_rel_err_plain"] < 0.2 and out["ke_max_rel_err_closure"] < 0.2
+
+
+def test_normalised_closure_features_and_stage():
+    """Scale-free mode: features 0..8 times feature 11 / delta give the raw gradients; the closure adds
+    -d_j [rho (g delta)^2 y_ij] with y the network's output on the normalised features."""
+    import torch
+
+    from public_b200.closure import ClosureMLP
+    s, q = cases.isotropic_turbulence(n=16, seed=3)
+    cfg = ocfg(s)
+    dx = cfg.dx()
+    delta = 0.3
+    with Cruna(Settings.from_dict(s)) as c, ClosureMLP(0, seed=4) as mlp:
+        mlp.params = M.init_params(7)
+        mlp.set_scaling(np.zeros(12), np.ones(12), np.full(6, 1e-2))
+        Xr = torch.empty((16 ** 3, 12), dtype=torch.float32, device="cuda")
+        Xn = torch.empty_like(Xr)
+        c.closure_features_dev(dev(flat(q)).data_ptr(), delta, Xr.data_ptr())
+        c.set_closure_normalisation(True)
+        c.closure_features_dev(dev(flat(q)).data_ptr(), delta, Xn.data_ptr())
+        c.sync()
+        y = mlp.forward(Xn).cpu().numpy().astype(np.float64)
+        plain = c.rhs_direct(q)
+        c.set_closure(mlp, delta)
+        with_cl = c.rhs_direct(q)
+        c.set_closure(None)
+    xr, xn = Xr.cpu().numpy().astype(np.float64), Xn.cpu().numpy().astype(np.float64)
+    g = np.sqrt(np.sum(xr[:, :9] ** 2, axis=1))
+    assert np.max(np.abs(xn[:, 11] - g * delta)) < 1e-5 * np.max(g * delta)
+    assert np.max(np.abs(xn[:, :9] * (xn[:, 11:12] / delta) - xr[:, :9])) < 1e-5 * np.max(np.abs(xr[:, :9]))
+    assert np.array_equal(xn[:, 9:11], xr[:, 9:11])
+    sc = xn[:, 9] * xn[:, 11] ** 2
+    T = [(y[:, t] * sc).reshape(q.shape[:3], order="F") for t in range(6)]
+    idx = {(0, 0): 0, (1, 1): 1, (2, 2): 2, (0, 1): 3, (1, 0): 3, (0, 2): 4, (2, 0): 4, (1, 2): 5, (2, 1): 5}
+    diff = with_cl - plain
+    for i in range(3):
+        div = sum(O.Dx(cfg, j, T[idx[(i, j)]], dx[j]) for j in range(3))
+        assert np.max(np.abs(diff[..., 1 + i] + div)) < 1e-9 * np.max(np.abs(div)) + 1e-12, i
