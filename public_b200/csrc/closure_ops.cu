@@ -134,14 +134,16 @@ void closure_stage(cruna_ctx *c, const double *q) {
   k_tau_fields<<<blocks, kThreads, 0, c->stream>>>(N, c->cl_y, c->cl_x, c->closure_norm ? 1 : 0, c->cl_tau);
   CRUNA_LAUNCH_CHECK(c);
   double *dtau = c->cl_tau + 6 * N;
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      if (c->dop[j].kind == OP_ZERO) {
+  for (int j = 0; j < 3; ++j) {  // d_j tau_ij of the three rows in one launch per direction
+    if (c->dop[j].kind == OP_ZERO) {
+      for (int i = 0; i < 3; ++i)
         CRUNA_CUDA_CHECK(cudaMemsetAsync(dtau + (i * 3 + j) * N, 0, sizeof(double) * N, c->stream));
-        continue;
-      }
-      apply_diff(c, j, c->cl_tau + tau_index(i, j) * N, nullptr, dtau + (i * 3 + j) * N, c->dx[j], 1);
+      continue;
     }
+    FieldSet fs;
+    for (int i = 0; i < 3; ++i) fs.add(c->cl_tau + tau_index(i, j) * N, nullptr, dtau + (i * 3 + j) * N);
+    apply_diff_set(c, j, fs, c->dx[j]);
+  }
   k_closure_force<<<blocks, kThreads, 0, c->stream>>>(N, c->user_force, dtau, c->cl_force);
   CRUNA_LAUNCH_CHECK(c);
   c->force = c->cl_force;

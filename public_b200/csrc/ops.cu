@@ -106,10 +106,9 @@ __device__ __forceinline__ double point_epilogue(const LineOp &op, double v, dou
 // one pointer; the KB results are formed before any is stored, so the loads of all KB points are in
 // flight together (and along z the shared taps are loaded once).  Other chunks take the generic path.
 template <int R, bool ANTI, int DIR, bool F2>
-__global__ void __launch_bounds__(128) k_line_stencil_r(LineOp op, Grid g, const double *__restrict__ f1,
-                                                        const double *__restrict__ f2,
-                                                        double *__restrict__ out, double scale, double sign,
-                                                        int nfields) {
+__global__ void __launch_bounds__(128) k_line_stencil_r(LineOp op, Grid g, const __grid_constant__ FieldSet fs,
+                                                        double scale, double sign) {
+  const int nfields = fs.n;
   constexpr int KB = 4;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= g.n1) return;
@@ -121,12 +120,14 @@ __global__ void __launch_bounds__(128) k_line_stencil_r(LineOp op, Grid g, const
   for (int zf = blockIdx.z; zf < nkb * nfields; zf += gridDim.z) {
     const int fld = zf / nkb, k0 = (zf - fld * nkb) * KB;
     const long long p0 = x + (long long)g.n1 * j + n12 * k0;
-    double *o = out + (long long)fld * g.N + p0;
+    const double *__restrict__ fa = fs.f1[fld];
+    const double *__restrict__ fb = F2 ? fs.f2[fld] : nullptr;
+    double *__restrict__ o = fs.out[fld] + p0;
     const int ilo = DIR == 0 ? x : (DIR == 1 ? j : k0), ihi = DIR == 2 ? k0 + KB - 1 : ilo;
     const int lo = op.periodic ? 0 : op.nb, hi = op.periodic ? n - 1 : n - 1 - op.nb;
     if (k0 + KB <= g.n3 && ilo - R >= 0 && ihi + R <= n - 1 && ilo >= lo && ihi <= hi) {
-      const double *a = f1 + (long long)fld * g.N + p0;
-      const double *b = F2 ? f2 + (long long)fld * g.N + p0 : nullptr;
+      const double *a = fa + p0;
+      const double *b = F2 ? fb + p0 : nullptr;
       double r[KB];
 #pragma unroll
       for (int u = 0; u < KB; ++u) {
@@ -145,8 +146,8 @@ __global__ void __launch_bounds__(128) k_line_stencil_r(LineOp op, Grid g, const
       const long long p = p0 + (k - k0) * n12;
       const int i = DIR == 0 ? x : (DIR == 1 ? j : k);
       const long long base = p - (long long)i * s;
-      const double *a = f1 + (long long)fld * g.N + base;
-      const double *b = F2 ? f2 + (long long)fld * g.N + base : nullptr;
+      const double *a = fa + base;
+      const double *b = F2 ? fb + base : nullptr;
       double v;
       if (op.periodic) {
         v = interior_part<R, ANTI>(op, [&](int m) {
@@ -330,6 +331,7 @@ __global__ void __launch_bounds__(64) k_line_compact_yz(LineOp op, Grid g, int d
 
 static size_t compact_smem(const LineOp &op) { return (size_t)op.n * (5 * sizeof(double) + sizeof(int)); }
 
+
 // the fast kernels handle interior radii 1..6 on lines longer than 2R + 2 (every periodic wrap then
 // stays within one period) whose open ends have at least R closure rows and an interior between them
 // (interior taps stay on the line)
@@ -339,34 +341,33 @@ static bool fast_ok(const LineOp &op) {
 }
 
 template <int R, bool ANTI, int DIR>
-static void launch_stencil_dir(cruna_ctx *c, const LineOp &op, const double *f1, const double *f2, double *out,
-                               double scale, double sign, int nfields) {
+static void launch_stencil_dir(cruna_ctx *c, const LineOp &op, const FieldSet &fs, double scale, double sign) {
   const int bx = c->g.n1 >= 128 ? 128 : (c->g.n1 >= 64 ? 64 : 32);
-  const dim3 grid((c->g.n1 + bx - 1) / bx, c->g.n2, std::min((c->g.n3 + 3) / 4 * nfields, 65535));
-  if (f2)
-    k_line_stencil_r<R, ANTI, DIR, true><<<grid, bx, 0, c->stream>>>(op, c->g, f1, f2, out, scale, sign, nfields);
+  const dim3 grid((c->g.n1 + bx - 1) / bx, c->g.n2, std::min((c->g.n3 + 3) / 4 * fs.n, 65535));
+  if (fs.f2[0])
+    k_line_stencil_r<R, ANTI, DIR, true><<<grid, bx, 0, c->stream>>>(op, c->g, fs, scale, sign);
   else
-    k_line_stencil_r<R, ANTI, DIR, false><<<grid, bx, 0, c->stream>>>(op, c->g, f1, f2, out, scale, sign, nfields);
+    k_line_stencil_r<R, ANTI, DIR, false><<<grid, bx, 0, c->stream>>>(op, c->g, fs, scale, sign);
 }
 
 template <int R, bool ANTI>
-static void launch_stencil_rr(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
-                              double *out, double scale, double sign, int nfields) {
-  if (dir == 0) launch_stencil_dir<R, ANTI, 0>(c, op, f1, f2, out, scale, sign, nfields);
-  else if (dir == 1) launch_stencil_dir<R, ANTI, 1>(c, op, f1, f2, out, scale, sign, nfields);
-  else launch_stencil_dir<R, ANTI, 2>(c, op, f1, f2, out, scale, sign, nfields);
+static void launch_stencil_rr(cruna_ctx *c, const LineOp &op, int dir, const FieldSet &fs, double scale,
+                              double sign) {
+  if (dir == 0) launch_stencil_dir<R, ANTI, 0>(c, op, fs, scale, sign);
+  else if (dir == 1) launch_stencil_dir<R, ANTI, 1>(c, op, fs, scale, sign);
+  else launch_stencil_dir<R, ANTI, 2>(c, op, fs, scale, sign);
 }
 
 template <bool ANTI>
-static void launch_stencil_r(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
-                             double *out, double scale, double sign, int nfields) {
+static void launch_stencil_r(cruna_ctx *c, const LineOp &op, int dir, const FieldSet &fs, double scale,
+                             double sign) {
   switch (op.r) {
-    case 1: launch_stencil_rr<1, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
-    case 2: launch_stencil_rr<2, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
-    case 3: launch_stencil_rr<3, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
-    case 4: launch_stencil_rr<4, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
-    case 5: launch_stencil_rr<5, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
-    case 6: launch_stencil_rr<6, ANTI>(c, op, dir, f1, f2, out, scale, sign, nfields); break;
+    case 1: launch_stencil_rr<1, ANTI>(c, op, dir, fs, scale, sign); break;
+    case 2: launch_stencil_rr<2, ANTI>(c, op, dir, fs, scale, sign); break;
+    case 3: launch_stencil_rr<3, ANTI>(c, op, dir, fs, scale, sign); break;
+    case 4: launch_stencil_rr<4, ANTI>(c, op, dir, fs, scale, sign); break;
+    case 5: launch_stencil_rr<5, ANTI>(c, op, dir, fs, scale, sign); break;
+    case 6: launch_stencil_rr<6, ANTI>(c, op, dir, fs, scale, sign); break;
   }
 }
 
@@ -375,15 +376,16 @@ static void launch_compact_r(cruna_ctx *c, const LineOp &op, int dir, const doub
                              double *out, double scale, double sign, int nfields) {
   const long long lines = (c->g.N / op.n) * nfields;
   const int blocks = nblocks(lines, 64);  // one line per thread: small blocks spread few lines over all SMs
+  const size_t sm = compact_smem(op);
   switch (op.r) {
 #define CRUNA_COMPACT_CASE(RR)                                                                          \
   case RR:                                                                                              \
     if (op.nopiv)                                                                                       \
-      k_line_compact_yz<RR, ANTI, true, true><<<blocks, 64, compact_smem(op), c->stream>>>(op, c->g, dir, f1, f2, out,   \
-                                                                            scale, sign, nfields);     \
+      k_line_compact_yz<RR, ANTI, true, true><<<blocks, 64, sm, c->stream>>>(op, c->g, dir, f1, f2, out, scale, \
+                                                                             sign, nfields);            \
     else                                                                                                \
-      k_line_compact_yz<RR, ANTI, true, false><<<blocks, 64, compact_smem(op), c->stream>>>(op, c->g, dir, f1, f2, out,  \
-                                                                             scale, sign, nfields);    \
+      k_line_compact_yz<RR, ANTI, true, false><<<blocks, 64, sm, c->stream>>>(op, c->g, dir, f1, f2, out, scale, \
+                                                                              sign, nfields);           \
     break;
     CRUNA_COMPACT_CASE(1) CRUNA_COMPACT_CASE(2) CRUNA_COMPACT_CASE(3)
     CRUNA_COMPACT_CASE(4) CRUNA_COMPACT_CASE(5) CRUNA_COMPACT_CASE(6)
@@ -391,41 +393,66 @@ static void launch_compact_r(cruna_ctx *c, const LineOp &op, int dir, const doub
   }
 }
 
+// contiguous fields f1 + k N (f2 + k N), out + k N, k < nfields, as field sets of at most kMax
+template <class F>
+static void for_sets(const cruna_ctx *c, const double *f1, const double *f2, double *out, int nfields, F &&fn) {
+  for (int k0 = 0; k0 < nfields; k0 += FieldSet::kMax) {
+    FieldSet fs;
+    for (int k = k0; k < std::min(nfields, k0 + FieldSet::kMax); ++k)
+      fs.add(f1 + (long long)k * c->g.N, f2 ? f2 + (long long)k * c->g.N : nullptr, out + (long long)k * c->g.N);
+    fn(fs);
+  }
+}
+
 static const char *const kStencilNames[2][3] = {{"line_filter_x", "line_filter_y", "line_filter_z"},
                                                 {"line_diff_x", "line_diff_y", "line_diff_z"}};
 
+static bool stencil_fast(const cruna_ctx *c, const LineOp &op) { return fast_ok(op) && c->g.n2 <= 65535; }
+static bool compact_fast(const LineOp &op, int dir) {
+  return op.kind == OP_STENCIL && op.solve && dir > 0 && fast_ok(op) && op.n <= kCompactMaxN;
+}
+
+static void launch_stencil_set(cruna_ctx *c, const LineOp &op, int dir, const FieldSet &fs, double scale,
+                               double sign) {
+  ProfScope ps(c, kStencilNames[op.antisym ? 1 : 0][dir]);
+  if (op.antisym) launch_stencil_r<true>(c, op, dir, fs, scale, sign);
+  else launch_stencil_r<false>(c, op, dir, fs, scale, sign);
+  CRUNA_LAUNCH_CHECK(c);
+}
+
 void launch_line_stencil(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
                          double *out, double scale, int nfields, double sign) {
-  ProfScope ps(c, kStencilNames[op.antisym ? 1 : 0][dir]);
-  if (fast_ok(op) && c->g.n2 <= 65535) {
-    if (op.antisym) launch_stencil_r<true>(c, op, dir, f1, f2, out, scale, sign, nfields);
-    else launch_stencil_r<false>(c, op, dir, f1, f2, out, scale, sign, nfields);
-  } else {
-    const long long work = c->g.N * nfields;
-    const int blocks = (int)std::min<long long>(nblocks(work), 148LL * 64);
-    k_line_stencil<<<blocks, kThreads, 0, c->stream>>>(op, c->g, dir, f1, f2, out, scale, sign, nfields);
+  if (stencil_fast(c, op)) {
+    for_sets(c, f1, f2, out, nfields, [&](const FieldSet &fs) { launch_stencil_set(c, op, dir, fs, scale, sign); });
+    return;
   }
+  ProfScope ps(c, kStencilNames[op.antisym ? 1 : 0][dir]);
+  const long long work = c->g.N * nfields;
+  const int blocks = (int)std::min<long long>(nblocks(work), 148LL * 64);
+  k_line_stencil<<<blocks, kThreads, 0, c->stream>>>(op, c->g, dir, f1, f2, out, scale, sign, nfields);
   CRUNA_LAUNCH_CHECK(c);
 }
 
 void launch_line_solve(cruna_ctx *c, const LineOp &op, int dir, double *data, int nfields) {
-  const long long lines = (c->g.N / op.n) * nfields;
   static const char *names[3] = {"line_solve_x", "line_solve_y", "line_solve_z"};
   ProfScope ps(c, names[dir]);
-  if (dir > 0 && op.n >= 4 && op.n <= kCompactMaxN && op.nopiv)
-    k_line_compact_yz<1, false, false, true><<<nblocks(lines, 64), 64, compact_smem(op), c->stream>>>(op, c->g, dir, nullptr,
-                                                                                       nullptr, data, 1.0, 1.0,
-                                                                                       nfields);
-  else if (dir > 0 && op.n >= 4 && op.n <= kCompactMaxN)
-    k_line_compact_yz<1, false, false, false><<<nblocks(lines, 64), 64, compact_smem(op), c->stream>>>(op, c->g, dir, nullptr,
-                                                                                        nullptr, data, 1.0, 1.0,
-                                                                                        nfields);
-  else
-    k_line_solve<<<nblocks(lines, 128), 128, 0, c->stream>>>(op, c->g, dir, data, nfields);
+  const long long lines = (c->g.N / op.n) * nfields;
+  if (dir > 0 && op.n >= 4 && op.n <= kCompactMaxN) {
+    if (op.nopiv)
+      k_line_compact_yz<1, false, false, true><<<nblocks(lines, 64), 64, compact_smem(op), c->stream>>>(
+          op, c->g, dir, nullptr, nullptr, data, 1.0, 1.0, nfields);
+    else
+      k_line_compact_yz<1, false, false, false><<<nblocks(lines, 64), 64, compact_smem(op), c->stream>>>(
+          op, c->g, dir, nullptr, nullptr, data, 1.0, 1.0, nfields);
+    CRUNA_LAUNCH_CHECK(c);
+    return;
+  }
+  k_line_solve<<<nblocks(lines, 128), 128, 0, c->stream>>>(op, c->g, dir, data, nfields);
   CRUNA_LAUNCH_CHECK(c);
 }
 
-// explicit part and compact solve of op along y or z in one pass (fast_ok(op), op.solve, dir > 0)
+// explicit part and compact solve of op along y or z in one pass (compact_fast(op, dir)) on nfields
+// contiguous fields
 static void launch_line_compact(cruna_ctx *c, const LineOp &op, int dir, const double *f1, const double *f2,
                                 double *out, double scale, int nfields) {
   static const char *names[2][3] = {{"", "compact_filter_y", "compact_filter_z"},
@@ -436,12 +463,27 @@ static void launch_line_compact(cruna_ctx *c, const LineOp &op, int dir, const d
   CRUNA_LAUNCH_CHECK(c);
 }
 
+// Dx_d of each field of a set (f1, or f1*f2 when every f2 is given), all with the same spacing h:
+// explicit operators take one launch per set; compact ones (whose kernel keeps one line per thread in
+// flight, so more fields per launch do not shorten it) and the fallbacks one apply_diff per field
+void apply_diff_set(cruna_ctx *c, int dir, const FieldSet &fs, double h) {
+  const LineOp &op = c->dop[dir];
+  const double scale = 1.0 / (h * op.div);
+  bool uniform = true;
+  for (int k = 1; k < fs.n; ++k) uniform = uniform && ((fs.f2[k] != nullptr) == (fs.f2[0] != nullptr));
+  if (uniform && !op.solve && stencil_fast(c, op)) {
+    launch_stencil_set(c, op, dir, fs, scale, 1.0);
+  } else {
+    for (int k = 0; k < fs.n; ++k) apply_diff(c, dir, fs.f1[k], fs.f2[k], fs.out[k], h, 1);
+  }
+}
+
 // Dx_d of f1 (or of f1*f2): explicit part scaled by 1/(h*div), then the compact solve if any
 void apply_diff(cruna_ctx *c, int dir, const double *f1, const double *f2, double *out, double h,
                 int nfields) {
   const LineOp &op = c->dop[dir];
   const double scale = 1.0 / (h * op.div);
-  if (op.kind == OP_STENCIL && op.solve && dir > 0 && fast_ok(op) && op.n <= kCompactMaxN) {
+  if (compact_fast(op, dir)) {
     launch_line_compact(c, op, dir, f1, f2, out, scale, nfields);
     return;
   }
@@ -453,7 +495,7 @@ void apply_diff(cruna_ctx *c, int dir, const double *f1, const double *f2, doubl
 void apply_filter(cruna_ctx *c, int dir, double *q, double *scratch, int nfields) {
   const LineOp &op = c->fop[dir];
   if (op.kind == OP_COPY) return;
-  if (op.kind == OP_STENCIL && op.solve && dir > 0 && fast_ok(op) && op.n <= kCompactMaxN) {
+  if (compact_fast(op, dir)) {
     launch_line_compact(c, op, dir, q, nullptr, scratch, 1.0, nfields);
   } else {
     launch_line_stencil(c, op, dir, q, nullptr, scratch, 1.0, nfields);
@@ -914,9 +956,12 @@ void rhs_direct_generic(cruna_ctx *c, const double *q_in, double *rhs, double *q
   k_prim<<<blocks, kThreads, 0, c->stream>>>(N, q, t, c->cfg.W / c->cfg.R);
   CRUNA_LAUNCH_CHECK(c);
   const double *dx = c->dx;
-  // velocity gradients (:102-112)
-  for (int v = 0; v < 3; ++v)
-    for (int d = 0; d < 3; ++d) apply_diff(c, d, F(F_U1 + v), nullptr, F(F_UX + 3 * v + d), dx[d], 1);
+  // velocity gradients (:102-112), the three components of one direction in one launch
+  for (int d = 0; d < 3; ++d) {
+    FieldSet fs;
+    for (int v = 0; v < 3; ++v) fs.add(F(F_U1 + v), nullptr, F(F_UX + 3 * v + d));
+    apply_diff_set(c, d, fs, dx[d]);
+  }
   // temperature gradient for the heat flux (:189-191), h absent unless heat_flux_dx
   for (int d = 0; d < 3; ++d)
     apply_diff(c, d, F(F_T), nullptr, F(F_TX + d), c->cfg.heat_flux_dx ? dx[d] : 1.0, 1);
@@ -933,11 +978,16 @@ void rhs_direct_generic(cruna_ctx *c, const double *q_in, double *rhs, double *q
   const int afl[3][3] = {{F_A1X, F_A1Y, F_A1Z}, {F_A2X, F_A2Y, F_A2Z}, {F_A3X, F_A3Y, F_A3Z}};
   const int vfl[3][3] = {{F_V1X, F_V1Y, F_V1Z}, {F_V2X, F_V2Y, F_V2Z}, {F_V3X, F_V3Y, F_V3Z}};
   const double *rq[3] = {ru, rv, rw};
-  for (int v = 0; v < 3; ++v) {
-    for (int d = 0; d < 3; ++d) apply_diff(c, d, rq[d], F(F_U1 + v), F(afl[v][d]), dx[d], 1);
-    apply_diff(c, v, pp, nullptr, F(F_PX + 7 * v), dx[v], 1);
-    for (int d = 0; d < 3; ++d) apply_diff(c, d, F(taus[v][d]), nullptr, F(vfl[v][d]), dx[d], 1);
+  for (int d = 0; d < 3; ++d) {  // per direction: the three fluxes rho u_d u_v, then the stresses tau_vd
+    FieldSet fl, st;
+    for (int v = 0; v < 3; ++v) {
+      fl.add(rq[d], F(F_U1 + v), F(afl[v][d]));
+      st.add(F(taus[v][d]), nullptr, F(vfl[v][d]));
+    }
+    apply_diff_set(c, d, fl, dx[d]);
+    apply_diff_set(c, d, st, dx[d]);
   }
+  for (int v = 0; v < 3; ++v) apply_diff(c, v, pp, nullptr, F(F_PX + 7 * v), dx[v], 1);
   // pressure flux (:180-182) and heat flux divergence (:195-197)
   for (int d = 0; d < 3; ++d) apply_diff(c, d, pp, F(F_U1 + d), F(F_EX + d), dx[d], 1);
   for (int d = 0; d < 3; ++d)
@@ -957,8 +1007,11 @@ void generic_forward_gradients(cruna_ctx *c, const double *q) {
   k_prim<<<blocks, kThreads, 0, c->stream>>>(N, q, t, c->cfg.W / c->cfg.R);
   CRUNA_LAUNCH_CHECK(c);
   const double *dx = c->dx;
-  for (int v = 0; v < 3; ++v)
-    for (int d = 0; d < 3; ++d) apply_diff(c, d, F(F_U1 + v), nullptr, F(F_UX + 3 * v + d), dx[d], 1);
+  for (int d = 0; d < 3; ++d) {
+    FieldSet fs;
+    for (int v = 0; v < 3; ++v) fs.add(F(F_U1 + v), nullptr, F(F_UX + 3 * v + d));
+    apply_diff_set(c, d, fs, dx[d]);
+  }
   for (int d = 0; d < 3; ++d)
     apply_diff(c, d, F(F_T), nullptr, F(F_TX + d), c->cfg.heat_flux_dx ? dx[d] : 1.0, 1);
   k_visc<<<blocks, kThreads, 0, c->stream>>>(N, t, c->cfg.mu0, c->cfg.T0,

@@ -126,6 +126,24 @@ inline long long offset_of(const cruna_ctx *c, const int sh[3]) {
   return sh[0] + (long long)c->g.n1 * (sh[1] + (long long)c->g.n2 * sh[2]);
 }
 
+// up to kMax fields of one line operator in one launch: out[f] = op(f1[f]) or op(f1[f] * f2[f])
+struct FieldSet {
+  static constexpr int kMax = 8;
+  const double *f1[kMax] = {};
+  const double *f2[kMax] = {};
+  double *out[kMax] = {};
+  int n = 0;
+  void add(const double *a, const double *b, double *o) {
+    f1[n] = a;
+    f2[n] = b;
+    out[n] = o;
+    ++n;
+  }
+};
+
+// Dx_d of every field of a set with spacing h (ops.cu): one launch where the fast line kernels apply
+void apply_diff_set(cruna_ctx *c, int dir, const FieldSet &fs, double h);
+
 // field slots of the generic RHS workspace (cruna_ctx::tmp)
 enum GenericField {
   F_U1, F_U2, F_U3, F_T,
