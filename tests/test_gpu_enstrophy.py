@@ -47,10 +47,11 @@ def test_diagnostics_match_oracle(case):
     assert abs(z - z_ref) < 1e-12 * abs(z_ref), (z, z_ref)
 
 
-@pytest.mark.parametrize("mode", [0, 1])
-def test_enstrophy_gradient_matches_oracle(mode):
+@pytest.mark.parametrize("mode,scheme", [(0, "o8_e_c_p"), (1, "o8_e_c_p"), (0, "o6_i_c_p"), (1, "o6_i_c_p")])
+def test_enstrophy_gradient_matches_oracle(mode, scheme):
     s, q = cases.taylor_green(n=12, seed=0)
     s["mu0"] = 0.02
+    s["diff"] = (scheme,) * 3
     S = O.Solver(ocfg(s), force=np.zeros_like(q))
     obj = {"kind": "enstrophy"}
     if mode == 0:
