@@ -685,6 +685,9 @@ __global__ void k_sponge(int mode, Grid g, SpongeDev sp, double gamma, double *a
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N;
        p += (long long)gridDim.x * blockDim.x) {
     const double sh = sponge_at(sp, g, p);
+    // outside the sponge layers the shape is exactly 0 and every update below leaves a unchanged
+    // (for finite values), so those points are not read or written
+    if (sh == 0.0) continue;
     const long long N = g.N;
     if (mode == 0) {          // rhs -= shape*(q - qref): a = rhs, b = q
       for (int v = 0; v < 5; ++v) a[p + v * N] = a[p + v * N] - sh * (b[p + v * N] - qref[p + v * N]);
