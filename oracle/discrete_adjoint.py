@@ -79,7 +79,7 @@ def _cs_vjp(fn, args, wrt, lam):
     return out
 
 
-def _apply_q_row(S: O.Solver, row, q: np.ndarray) -> np.ndarray:
+def _apply_q_row(S: O.Solver, row, q: np.ndarray, outside_rhs: bool = False) -> np.ndarray:
     """One row of set_boundary_condition_q (boundary_conditions.f90:52-136), as the oracle applies it."""
     cfg = S.cfg
     t = int(round(row[0]))
@@ -91,19 +91,24 @@ def _apply_q_row(S: O.Solver, row, q: np.ndarray) -> np.ndarray:
         q[b] = O.characteristic_q_k1d(cfg, q[b], q[b2], row[7:10])
     elif t == 201:
         q[b] = O.characteristic_q_k1d(cfg, q[b], S.qref[b], row[7:10])
+    elif t == 202:
+        q[b] = O.characteristic_q_k1d(cfg, q[b], S.qref[b], S.kvec[b])
+    elif t == 203 and O._zonal_active(row, outside_rhs):
+        q = O.characteristic_q_k1d(cfg, q, S.qref, S.kvec, S.shape)
     elif t == 401:
         for v in range(5):
             q[..., v] = q[..., v] - S.shape * (q[..., v] - S.qref[..., v])
     return q
 
 
-def bc_q_vjp(S: O.Solver, q_in: np.ndarray, lam: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
-    """Transpose of set_boundary_condition_q at q_in; returns (lam_in, q after the BC)."""
+def bc_q_vjp(S: O.Solver, q_in: np.ndarray, lam: np.ndarray,
+             outside_rhs: bool = False) -> Tuple[np.ndarray, np.ndarray]:
+    """Transpose of set_boundary_condition_q(q, outside_rhs) at q_in; returns (lam_in, q after the BC)."""
     states = []
     q = q_in
     for row in S.bc:
         states.append(q)
-        q = _apply_q_row(S, row, q)
+        q = _apply_q_row(S, row, q, outside_rhs)
     lam = lam.copy(order="F")
     cfg = S.cfg
     for row, qpre in zip(S.bc[::-1], states[::-1]):
@@ -112,6 +117,12 @@ def bc_q_vjp(S: O.Solver, q_in: np.ndarray, lam: np.ndarray) -> Tuple[np.ndarray
         k = row[7:10]
         if t == 401:
             lam = lam * (1.0 - S.shape)[..., None]
+        elif t == 202:
+            fn = lambda qq: O.characteristic_q_k1d(cfg, qq, S.qref[b], S.kvec[b])
+            lam[b] = _cs_vjp(fn, [qpre[b]], 0, lam[b])
+        elif t == 203 and O._zonal_active(row, outside_rhs):
+            fn = lambda qq: O.characteristic_q_k1d(cfg, qq, S.qref, S.kvec, S.shape)
+            lam = _cs_vjp(fn, [qpre], 0, lam)
         elif t == 201:
             fn = lambda qq: O.characteristic_q_k1d(cfg, qq, S.qref[b], k)
             lam[b] = _cs_vjp(fn, [qpre[b]], 0, lam[b])
@@ -137,12 +148,12 @@ def bc_rhs_vjp(S: O.Solver, qb: np.ndarray, lam: np.ndarray) -> Tuple[np.ndarray
     """Transpose of set_boundary_condition_rhs(rhs, qb) (boundary_conditions.f90:228-298):
     returns (cotangent of the RHS before the BC, cotangent of qb)."""
     cfg = S.cfg
-    rows = [r for r in S.bc if int(round(r[0])) in (100, 204, 400)]
+    rows = [r for r in S.bc if int(round(r[0])) in (100, 204, 205, 206, 400)]
     lam_q = np.zeros_like(qb)
     if not rows:
         return lam.copy(order="F"), lam_q
     pre = []
-    if any(int(round(r[0])) == 204 for r in rows):
+    if any(int(round(r[0])) in (204, 205, 206) for r in rows):
         rhs = _rhs_pre_bc(S, qb)
         for row in rows:
             pre.append(rhs.copy())
@@ -152,6 +163,10 @@ def bc_rhs_vjp(S: O.Solver, qb: np.ndarray, lam: np.ndarray) -> Tuple[np.ndarray
                 rhs[b + (int(round(row[7])) - 1,)] = 0.0
             elif t == 204:
                 rhs[b] = O.characteristic_rhs_k1d(cfg, rhs[b], qb[b], S.qref[b], row[7:10])
+            elif t == 205:
+                rhs[b] = O.characteristic_rhs_k1d(cfg, rhs[b], qb[b], S.qref[b], S.kvec[b])
+            elif t == 206:
+                rhs = O.characteristic_rhs_k1d(cfg, rhs, qb, S.qref, S.kvec, S.shape)
             else:
                 for v in range(5):
                     rhs[..., v] = rhs[..., v] - S.shape * (qb[..., v] - S.qref[..., v])
@@ -165,6 +180,16 @@ def bc_rhs_vjp(S: O.Solver, qb: np.ndarray, lam: np.ndarray) -> Tuple[np.ndarray
             lam[b + (int(round(row[7])) - 1,)] = 0.0
         elif t == 400:
             lam_q = lam_q - S.shape[..., None] * lam
+        elif t == 205:
+            fn = lambda rr, qq: O.characteristic_rhs_k1d(cfg, rr, qq, S.qref[b], S.kvec[b])
+            lb = lam[b].copy()
+            lam_q[b] = lam_q[b] + _cs_vjp(fn, [rpre[b], qb[b]], 1, lb)
+            lam[b] = _cs_vjp(fn, [rpre[b], qb[b]], 0, lb)
+        elif t == 206:
+            fn = lambda rr, qq: O.characteristic_rhs_k1d(cfg, rr, qq, S.qref, S.kvec, S.shape)
+            lb = lam.copy()
+            lam_q = lam_q + _cs_vjp(fn, [rpre, qb], 1, lb)
+            lam = _cs_vjp(fn, [rpre, qb], 0, lb)
         else:
             k = row[7:10]
             fn = lambda rr, qq: O.characteristic_rhs_k1d(cfg, rr, qq, S.qref[b], k)
@@ -262,8 +287,6 @@ def rhs_interior_vjp(S: O.Solver, q: np.ndarray, lam: np.ndarray) -> np.ndarray:
 
 def rhs_vjp(S: O.Solver, q_in: np.ndarray, lam: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
     """(d rhs_direct/d q)^T lam at q_in, and the cotangent of the forcing (d rhs/d f)^T lam."""
-    if any(int(round(r[0])) in (202, 203, 205, 206) for r in S.bc):
-        raise NotImplementedError("the zonal BC types are not transposed")
     _, qb = bc_q_vjp(S, q_in, np.zeros_like(q_in))
     lam_pre, lam_qb = bc_rhs_vjp(S, qb, lam)
     lam_qb = lam_qb + rhs_interior_vjp(S, qb, lam_pre)
@@ -302,7 +325,7 @@ def step_vjp(S: O.Solver, q0: np.ndarray, lam1: np.ndarray, nt: int) -> Tuple[np
     for d in (2, 1, 0):
         if nt % cfg.di_freq[d] == 0:
             lam = filter_T(cfg, d, lam)
-    lam_q1, _ = bc_q_vjp(S, q1, lam)
+    lam_q1, _ = bc_q_vjp(S, q1, lam, outside_rhs=True)
     lk = dt / 6.0 * lam_q1
     mu4, f4 = rhs_vjp(S, Q4, lk)
     lk = dt / 3.0 * lam_q1 + dt * mu4

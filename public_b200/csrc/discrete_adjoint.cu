@@ -285,6 +285,69 @@ __global__ void k_char_rhs_T(Box b, Grid g, double k1, double k2, double k3, dou
   }
 }
 
+// zonal types 202 (shape 1) and 203 (shape-weighted): aim = qref, the boundary normal from the
+// k-vector field (nonreflecting.f90:141-233)
+__global__ void k_char_q4_T(Box b, Grid g, const double *__restrict__ kv, SpongeDev sp, int shaped, double gamma,
+                            const double *save, const double *qref, double *lam) {
+  const long long tot = b.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    const long long p = box_point(b, g, t, i, j, k);
+    const long long N = g.N;
+    Dual<5> qd[5], out[5];
+    double av[5], l[5];
+    for (int v = 0; v < 5; ++v) {
+      qd[v] = Dual<5>::seed(save[t * 10 + v], v);
+      av[v] = qref[p + v * N];
+      l[v] = lam[p + v * N];
+    }
+    char_q_point(qd, av, kv[p], kv[p + N], kv[p + 2 * N], gamma, out, shaped ? sponge_at(sp, g, p) : 1.0);
+    for (int jj = 0; jj < 5; ++jj) {
+      double sum = 0.0;
+      for (int v = 0; v < 5; ++v) sum += l[v] * out[v].d[jj];
+      lam[p + jj * N] = sum;
+    }
+  }
+}
+
+// zonal types 205 and 206 on the RHS (nonreflecting.f90:345-449): rhs and q differentiated
+__global__ void k_char_rhs4_T(Box b, Grid g, const double *__restrict__ kv, SpongeDev sp, int shaped,
+                              double gamma, double dt, const double *save, const double *qb, const double *qref,
+                              double *lam, double *lam_q) {
+  const long long tot = b.count();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    const long long p = box_point(b, g, t, i, j, k);
+    const long long N = g.N;
+    Dual<10> rd[5], qd[5], out[5];
+    double av[5], l[5];
+    for (int v = 0; v < 5; ++v) {
+      rd[v] = Dual<10>::seed(save[t * 10 + v], v);
+      qd[v] = Dual<10>::seed(qb[p + v * N], 5 + v);
+      av[v] = qref[p + v * N];
+      l[v] = lam[p + v * N];
+    }
+    char_rhs_point(rd, qd, av, kv[p], kv[p + N], kv[p + 2 * N], gamma, dt, out, shaped != 0,
+                   shaped ? sponge_at(sp, g, p) : 0.0);
+    for (int jj = 0; jj < 5; ++jj) {
+      double sr = 0.0, sq = 0.0;
+      for (int v = 0; v < 5; ++v) {
+        sr += l[v] * out[v].d[jj];
+        sq += l[v] * out[v].d[5 + jj];
+      }
+      lam[p + jj * N] = sr;
+      lam_q[p + jj * N] += sq;
+    }
+  }
+}
+
+// the q-BC rows that act in this call: type 203 only inside or only outside the RHS (r.only)
+bool q_row_active(const BCRow &r, int outside) {
+  return r.type != 203 || (outside ? r.only != 1 : r.only != -1);
+}
+
 // mode 0: lam *= (1 - shape) (transpose of the type 401 sponge on q); mode 1: lam_q -= shape * lam
 // (type 400 sponge on the RHS, sponge_layer_core.f90:45-48 and :80-84)
 __global__ void k_sponge_T(int mode, Grid g, SpongeDev sp, double *a, const double *b) {
@@ -323,33 +386,38 @@ void with_single_row(cruna_ctx *c, const BCRow &row, F &&f) {
   std::swap(c->bc, one);
 }
 
-// replays set_boundary_condition_q (boundary_conditions.f90:52-136) on a copy of q, row by row as the
-// direct path applies them, saving each characteristic row's box input; returns the post-BC state
-double *bc_q_replay(cruna_ctx *c, const double *q) {
+// replays set_boundary_condition_q(q, outside) (boundary_conditions.f90:52-136) on a copy of q, row
+// by row as the direct path applies them, saving each characteristic row's box input; returns the
+// post-BC state
+double *bc_q_replay(cruna_ctx *c, const double *q, int outside) {
   double *qr = c->vjp_st[S_QREP];
   copy_state(c, qr, q, 5);
   for (size_t r = 0; r < c->bc.size(); ++r) {
     const BCRow &row = c->bc[r];
     Box b = box_of(row);
-    if (row.type == 200 || row.type == 201) {
+    if (row.type == 200 || row.type == 201 || row.type == 202 || (row.type == 203 && q_row_active(row, outside))) {
       const long long off = row.type == 200 ? offset_of(c, row.shift) : 0;
       k_pack<<<nblocks(b.count()), kThreads, 0, c->stream>>>(b, c->g, qr, row.type == 200 ? qr : nullptr, off,
                                                               c->vjp_save[r]);
       CRUNA_LAUNCH_CHECK(c);
     }
     const BCRow copy = row;
-    with_single_row(c, copy, [&]() { bc_q(c, qr, 0); });
+    with_single_row(c, copy, [&]() { bc_q(c, qr, outside); });
   }
   return qr;
 }
 
-// transpose of set_boundary_condition_q, in place on lam, using the saves of the last replay
-void bc_q_T(cruna_ctx *c, double *lam) {
+// transpose of set_boundary_condition_q(., outside), in place on lam, using the saves of the last replay
+void bc_q_T(cruna_ctx *c, double *lam, int outside) {
   for (size_t rr = c->bc.size(); rr-- > 0;) {
     const BCRow &row = c->bc[rr];
     Box b = box_of(row);
     const int blocks = nblocks(b.count());
-    if (row.type == 401) {
+    if (row.type == 202 || (row.type == 203 && q_row_active(row, outside))) {
+      k_char_q4_T<<<blocks, kThreads, 0, c->stream>>>(b, c->g, c->kvec, c->sponge, row.type == 203, c->cfg.gamma,
+                                                      c->vjp_save[rr], c->qref, lam);
+      CRUNA_LAUNCH_CHECK(c);
+    } else if (row.type == 401) {
       k_sponge_T<<<nblocks(c->g.N), kThreads, 0, c->stream>>>(0, c->g, c->sponge, lam, nullptr);
       CRUNA_LAUNCH_CHECK(c);
     } else if (row.type == 201) {
@@ -367,15 +435,16 @@ void bc_q_T(cruna_ctx *c, double *lam) {
 // transpose of set_boundary_condition_rhs(rhs, qb) (boundary_conditions.f90:228-298): lam is the
 // RHS cotangent (in place: becomes the cotangent before the BC), lam_q receives the qb cotangent
 void bc_rhs_T(cruna_ctx *c, const double *qb, double *lam, double *lam_q) {
-  bool any204 = false;
-  for (const BCRow &r : c->bc) any204 = any204 || r.type == 204;
-  if (any204) {  // replay on the RHS before the BC, saving each type-204 box input
+  auto characteristic = [](int type) { return type == 204 || type == 205 || type == 206; };
+  bool any = false;
+  for (const BCRow &r : c->bc) any = any || characteristic(r.type);
+  if (any) {  // replay on the RHS before the BC, saving each characteristic row's box input
     double *R = c->vjp_st[S_K];
     rhs_direct_generic(c, qb, R, c->st[4], 0);
     for (size_t r = 0; r < c->bc.size(); ++r) {
       const BCRow &row = c->bc[r];
       Box b = box_of(row);
-      if (row.type == 204) {
+      if (characteristic(row.type)) {
         k_pack<<<nblocks(b.count()), kThreads, 0, c->stream>>>(b, c->g, R, nullptr, 0, c->vjp_save[r]);
         CRUNA_LAUNCH_CHECK(c);
       }
@@ -395,6 +464,10 @@ void bc_rhs_T(cruna_ctx *c, const double *qb, double *lam, double *lam_q) {
       CRUNA_LAUNCH_CHECK(c);
     } else if (row.type == 204) {
       k_char_rhs_T<<<blocks, kThreads, 0, c->stream>>>(b, c->g, row.k[0], row.k[1], row.k[2], c->cfg.gamma,
+                                                        c->cfg.dt, c->vjp_save[rr], qb, c->qref, lam, lam_q);
+      CRUNA_LAUNCH_CHECK(c);
+    } else if (row.type == 205 || row.type == 206) {
+      k_char_rhs4_T<<<blocks, kThreads, 0, c->stream>>>(b, c->g, c->kvec, c->sponge, row.type == 206, c->cfg.gamma,
                                                         c->cfg.dt, c->vjp_save[rr], qb, c->qref, lam, lam_q);
       CRUNA_LAUNCH_CHECK(c);
     }
@@ -556,9 +629,6 @@ void ensure_vjp(cruna_ctx *c) {
     throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint transposes the FP64 operator: precision must be FP64"};
   if (c->closure_mlp) throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint does not transpose the closure"};
   if (c->halo_fn) throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint runs on one block (no z slabs)"};
-  for (const BCRow &r : c->bc)
-    if (r.type >= 202 && r.type <= 206 && r.type != 204)
-      throw ApiError{CRUNA_ERR_UNSUPPORTED, "the discrete adjoint does not transpose the zonal BC types 202/203/205/206"};
   for (int d = 0; d < 3; ++d) {
     if (!c->dopT_built[d]) build_transpose(c, c->dop[d], c->dhf[d], c->dopT[d]);
     c->dopT_built[d] = true;
@@ -569,7 +639,7 @@ void ensure_vjp(cruna_ctx *c) {
   c->vjp_save.assign(c->bc.size(), nullptr);
   for (size_t r = 0; r < c->bc.size(); ++r) {
     const BCRow &row = c->bc[r];
-    if (row.type == 200 || row.type == 201 || row.type == 204)
+    if (row.type >= 200 && row.type <= 206)
       c->vjp_save[r] = dalloc(c, (size_t)box_of(row).count() * 10);
   }
   ensure_generic(c);
@@ -584,7 +654,7 @@ bool due_at(int freq, int nt) { return freq > 0 && nt % freq == 0; }
 // (d rhs_direct / d q)^T lam at q; gf_acc (optional) += (d rhs / d f)^T lam
 void rhs_direct_vjp(cruna_ctx *c, const double *q, const double *lam, double *mu, double *gf_acc) {
   ensure_vjp(c);
-  const double *qb = c->has_q_bc ? bc_q_replay(c, q) : q;
+  const double *qb = c->has_q_bc ? bc_q_replay(c, q, 0) : q;
   double *lpre = c->vjp_st[S_LPRE], *lq = c->vjp_st[S_LQ];
   copy_state(c, lpre, lam, 5);
   if (c->has_rhs_bc) {
@@ -593,7 +663,7 @@ void rhs_direct_vjp(cruna_ctx *c, const double *q, const double *lam, double *mu
   }
   if (gf_acc) add_fields(c, gf_acc, lpre, c->g.N * 5);
   interior_vjp(c, qb, lpre, mu, c->has_rhs_bc ? lq : nullptr);
-  if (c->has_q_bc) bc_q_T(c, mu);
+  if (c->has_q_bc) bc_q_T(c, mu, 0);
 }
 
 // transpose of one calc_direct loop step nt at q0: lam0 = (d q1 / d q0)^T lam1, gf_acc += (d q1/d f)^T lam1
@@ -627,8 +697,8 @@ void step_direct_vjp(cruna_ctx *c, const double *q0, const double *lam1, double 
   for (int d = 2; d >= 0; --d)
     if (due_at(c->cfg.di_freq[d], nt)) filter_T(c, d, l1, k);
   if (c->has_q_bc) {
-    bc_q_replay(c, S[S_Q1]);
-    bc_q_T(c, l1);
+    bc_q_replay(c, S[S_Q1], 1);
+    bc_q_T(c, l1, 1);
   }
   // RK4 transposed: lam0 = l1 + sum_s J_s^T lk_s, stages in reverse order
   copy_state(c, lam0, l1, 5);

@@ -179,3 +179,39 @@ def test_enstrophy_gradient_through_steps():
     _, gfc, gqc = O.gradient_store_all(S, q, 3, {"kind": "enstrophy"})
     cos = float(np.sum(gqc * gqd) / np.linalg.norm(gqc) / np.linalg.norm(gqd))
     assert cos > 0.9999, cos
+
+
+ZONAL_ROWS = {
+    "202": [[202, 1, 10, 1, 1, 1, 12, 0, 0, 0], [202, 10, 10, 1, 11, 1, 12, 0, 0, 0]],
+    "203": [[203, 1, 10, 1, 11, 1, 12, 0, 0, 0]],
+    "203in": [[203, 1, 10, 1, 11, 1, 12, 1, 0, 0]],
+    "203out": [[203, 1, 10, 1, 11, 1, 12, -1, 0, 0]],
+    "205": [[205, 1, 10, 11, 11, 1, 12, 0, 0, 0]],
+    "206": [[206, 1, 10, 1, 11, 1, 12, 0, 0, 0]],
+}
+
+
+def zonal_case(kind, kv="hedgehog", scheme="o4_e_c_o"):
+    n = (10, 11, 12)
+    q = cases.smooth_random_state(n, seed=7, p0=1.0, rho0=1.0, amp=0.05)
+    qref = cases.smooth_random_state(n, seed=8, p0=1.0, rho0=1.0, amp=0.05)
+    s = dict(n=n, diff=(scheme,) * 3, x1=(1.0, 1.2, 1.4), dt=1e-3, bc=np.array(ZONAL_ROWS[kind], dtype=float),
+             sponge_length=(0.2, 0.3, 0.25), sponge_amplitude=0.8, R=1.0, W=1.0, T0=1.0, mu0=0.01, kvector=kv)
+    return s, q, qref
+
+
+@pytest.mark.parametrize("kind", sorted(ZONAL_ROWS))
+def test_rhs_transpose_zonal_boundaries(kind):
+    """Zonal characteristic types 202/203 (on q) and 205/206 (on the RHS): <lam, J v> = <J^T lam, v>."""
+    s, q, qref = zonal_case(kind)
+    S = O.Solver(ocfg(s), qref=qref)
+    assert rhs_dot_mismatch(S, q, eps=1e-7) < 1e-7, kind
+
+
+@pytest.mark.parametrize("kind", ["203out", "206"])
+def test_step_transpose_zonal_boundaries(kind):
+    """One loop step (RK4, the outside-RHS boundary update, filters) against central differences of J."""
+    s, q, qref = zonal_case(kind, kv="diagonal")
+    S = O.Solver(ocfg(s), qref=qref, force=np.zeros_like(q))
+    eq, ef = grad_mismatch(S, q, 2, {"kind": "kinetic_energy"}, eps=1e-7)
+    assert eq < 1e-6 and ef < 1e-6, (eq, ef)

@@ -199,3 +199,39 @@ def test_optimisation_loop_matches_oracle(mode):
     assert np.allclose(ag, ar, rtol=1e-7, atol=0), (ag, ar)
     assert cot_err(fg, fr) < 1e-8, cot_err(fg, fr)
     assert Jg[-1] < 0.5 * Jg[0]
+
+
+ZONAL_ROWS = {
+    "202": [[202, 1, 10, 1, 1, 1, 12, 0, 0, 0], [202, 10, 10, 1, 11, 1, 12, 0, 0, 0]],
+    "203": [[203, 1, 10, 1, 11, 1, 12, 0, 0, 0]],
+    "203in": [[203, 1, 10, 1, 11, 1, 12, 1, 0, 0]],
+    "203out": [[203, 1, 10, 1, 11, 1, 12, -1, 0, 0]],
+    "205": [[205, 1, 10, 11, 11, 1, 12, 0, 0, 0]],
+    "206": [[206, 1, 10, 1, 11, 1, 12, 0, 0, 0]],
+}
+
+
+@pytest.mark.parametrize("kv", ["diagonal", "hedgehog"])
+@pytest.mark.parametrize("kind", sorted(ZONAL_ROWS))
+def test_rhs_and_step_vjp_zonal_boundaries_match_oracle(kind, kv):
+    """Zonal characteristic types (normal vectors from the k-vector field, 203/206 weighted by the
+    sponge shape, 203 inside and/or outside the RHS): RHS transpose and one loop step transposed."""
+    n = (10, 11, 12)
+    q = cases.smooth_random_state(n, seed=7, p0=1.0, rho0=1.0, amp=0.05)
+    qref = cases.smooth_random_state(n, seed=8, p0=1.0, rho0=1.0, amp=0.05)
+    f = cases.smooth_random_state(n, seed=5, p0=0.0, rho0=0.0, amp=1.0)
+    s = dict(n=n, diff=("o4_e_c_o",) * 3, x1=(1.0, 1.2, 1.4), dt=1e-3, bc=np.array(ZONAL_ROWS[kind], dtype=float),
+             sponge_length=(0.2, 0.3, 0.25), sponge_amplitude=0.8, R=1.0, W=1.0, T0=1.0, mu0=0.01, kvector=kv)
+    S = O.Solver(ocfg(s), qref=qref, force=f)
+    lam = rnd(q.shape, 4)
+    mu_ref, gf_ref = DA.rhs_vjp(S, q, lam)
+    l0_ref, gs_ref = DA.step_vjp(S, q, lam, 1)
+    with Cruna(Settings.from_dict(s), qref=qref, force=f) as c:
+        gf = np.zeros_like(q, order="F")
+        mu = c.rhs_direct_vjp(q, lam, gf)
+        gs = np.zeros_like(q, order="F")
+        l0 = c.step_direct_vjp(q, lam, 1, gs)
+    assert cot_err(mu, mu_ref) < TOL, cot_err(mu, mu_ref)
+    assert cot_err(gf, gf_ref) < TOL, cot_err(gf, gf_ref)
+    assert cot_err(l0, l0_ref) < TOL, cot_err(l0, l0_ref)
+    assert cot_err(gs, gs_ref) < TOL, cot_err(gs, gs_ref)
