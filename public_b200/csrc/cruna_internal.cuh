@@ -11,6 +11,8 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/cruna_b200.h"
 
 namespace cruna {
@@ -248,11 +250,16 @@ void add_fields(cruna_ctx *c, double *dst, const double *src, long long n);
 int prof_begin(cruna_ctx *c, const char *name);
 void prof_end(cruna_ctx *c, int idx);
 void prof_drain(cruna_ctx *c);
+// one kernel family's launch: an NVTX range on the host (visible to a timeline profiler; the calls
+// do nothing without one) and, while kernel timing is on, CUDA events on the context's stream
 struct ProfScope {
   cruna_ctx *c;
   int idx;
-  ProfScope(cruna_ctx *ctx, const char *name) : c(ctx), idx(prof_begin(ctx, name)) {}
-  ~ProfScope() { prof_end(c, idx); }
+  ProfScope(cruna_ctx *ctx, const char *name) : c(ctx), idx(prof_begin(ctx, name)) { nvtxRangePushA(name); }
+  ~ProfScope() {
+    prof_end(c, idx);
+    nvtxRangePop();
+  }
 };
 
 }  // namespace cruna

@@ -96,3 +96,14 @@ def test_device_loop_with_torch_buffers():
         cap, rep = c.graph_stats()
     assert np.array_equal(got, ref)
     assert cap == 4 and rep == 32             # two calls, each: 2 eager, 2 recorded, 16 replays
+
+
+def test_restart_from_an_intermediate_step_is_bit_identical():
+    """cruna_run_direct from nt0 continues a run exactly (the filter pattern follows the global step
+    count), like a restart from (subset, step) in the reference's cruna_hpc.f90:109-148."""
+    s, q = tgv_settings()
+    with Cruna(Settings.from_dict(s), qref=q) as c:
+        whole = c.calc_direct(q, 11)
+        part = c.calc_direct(q, 4)
+        rest = c.calc_direct(part, 7, nt0=4)
+    assert np.array_equal(whole, rest)
