@@ -22,6 +22,7 @@ import math
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -31,7 +32,8 @@ sys.path.insert(0, ROOT)
 METRIC = "point-steps/s direct+adjoint"
 UNIT = "point-steps/s"
 
-# algorithmic HBM bytes per grid point and launch of each kernel family (FP64 state)
+# algorithmic HBM bytes per grid point and launch of each kernel family (FP64 state): the compulsory
+# reads and writes of one launch
 ALG_BYTES_FP64 = {
     "pass_g": 40 + 15 * 8,          # read q, write 15 fields
     "pass_d": 9 * 8 + 6 * 8 + 140,  # read 9 stencil fields + 6 centre fields, RK stage I/O (average)
@@ -115,7 +117,9 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        # raw samples (the JSON line carries their summary); CRUNA_CLOCKS_DIR keeps them elsewhere
+        self.path = os.path.join(os.environ.get("CRUNA_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"clocks_bench_{os.getpid()}.csv")
 
     def start(self):
         try:

@@ -1,6 +1,6 @@
 """CPU oracle for the CRUNA direct + adjoint Navier-Stokes time step (TEST INFRASTRUCTURE).
 
-This module is the checker, never the product: only ``tests/``, ``__graft_entry__.smoke()`` and the
+This module is test infrastructure, never the product: only ``tests/``, ``__graft_entry__.smoke()`` and the
 ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may import it.  The shipped path is the
 CUDA library in ``public_b200/csrc`` and fails loudly when that library is missing.
 

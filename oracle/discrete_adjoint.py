@@ -1,5 +1,5 @@
-"""Exact discrete adjoint of the direct time step (TEST INFRASTRUCTURE: the checker of the library's
-discrete-adjoint entry points; only ``tests/`` may import it).
+"""Exact discrete adjoint of the direct time step (TEST INFRASTRUCTURE: the reference the tests hold
+the library's discrete-adjoint entry points against; only ``tests/`` may import it).
 
 The reference has no discrete adjoint: its adjoint (src/equations/ns_rho_rhou_p.f90:257-536) is the
 continuous inviscid adjoint, which is not the transpose of the discrete direct operator.  This module

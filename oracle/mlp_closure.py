@@ -1,5 +1,5 @@
-"""CPU reference of the subgrid-closure MLP (TEST INFRASTRUCTURE: the checker of the library's
-tensor-core MLP kernels; only ``tests/`` and the closure study's CPU comparison may import it).
+"""CPU reference of the subgrid-closure MLP (TEST INFRASTRUCTURE: the reference the tests hold the
+library's tensor-core MLP kernels against; only ``tests/`` may import it).
 
 The closure has no counterpart in the reference (CRUNA has no learned component).  The network maps
 12 features (9 velocity-gradient components, density, temperature, filter width; normalised by a

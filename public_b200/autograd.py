@@ -1,5 +1,5 @@
-"""torch.autograd wrapper of the solver's objective gradient (the role of CRUNA's ext/python layer in
-this build: PyTorch drives training and gradient checks, the solver runs in libcruna_b200.so).
+"""torch.autograd wrapper of the solver's objective gradient (the role of CRUNA's ext/python layer
+here: PyTorch drives training and gradient checks, the solver runs in libcruna_b200.so).
 
 ``CrunaObjective.apply(q0, f, solver, nsteps, nsnap, objective)`` returns the scalar objective J of
 ``nsteps`` direct steps started from ``q0`` with the time-constant forcing ``f`` (both CUDA float64
