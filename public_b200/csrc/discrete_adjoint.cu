@@ -158,6 +158,41 @@ __global__ void k_band_T(LineOpT op, Grid g, int dir, const double *__restrict__
   }
 }
 
+// the same banded product with the line position from the launch grid (x = block x range, y = j,
+// (k, field) = z, strided) instead of a division per point; DIR is compile-time
+template <int DIR>
+__global__ void __launch_bounds__(128) k_band_T_grid(LineOpT op, Grid g, const double *__restrict__ in,
+                                                     double *__restrict__ out, double scale, int nfields,
+                                                     int accumulate) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= g.n1) return;
+  const int j = blockIdx.y;
+  const int n = op.n, w = op.hi - op.lo + 1;
+  const long long n12 = (long long)g.n1 * g.n2;
+  const long long s = DIR == 0 ? 1 : (DIR == 1 ? (long long)g.n1 : n12);
+  for (int kf = blockIdx.z; kf < g.n3 * nfields; kf += gridDim.z) {
+    const int fld = kf / g.n3, k = kf - fld * g.n3;
+    const long long p = x + (long long)g.n1 * j + n12 * k;
+    const int i = DIR == 0 ? x : (DIR == 1 ? j : k);
+    const double *a = in + (long long)fld * g.N + p - (long long)i * s;  // the line's first point
+    const double *__restrict__ row = op.band + (long long)i * w;
+    double v = 0.0;
+    for (int o = op.lo; o <= op.hi; ++o) {
+      int jj = i + o;
+      if (op.periodic) {
+        if (jj < 0) jj += n;
+        else if (jj >= n) jj -= n;
+      } else if (jj < 0 || jj >= n) {
+        continue;
+      }
+      v += row[o - op.lo] * a[jj * s];
+    }
+    v *= scale;
+    double *o_ = out + (long long)fld * g.N + p;
+    *o_ = accumulate ? *o_ + v : v;
+  }
+}
+
 // out (+)= scale * A^T B^-T in, on nfields fields along dir
 void apply_T(cruna_ctx *c, const LineOpT &t, int dir, const double *in, double *out, double scale, int nfields,
              int accumulate, double *scratch) {
@@ -178,8 +213,16 @@ void apply_T(cruna_ctx *c, const LineOpT &t, int dir, const double *in, double *
     src = scratch;
   }
   ProfScope ps(c, "band_T");
-  k_band_T<<<(int)std::min<long long>(nblocks(M), 148LL * 64), kThreads, 0, c->stream>>>(
-      t, c->g, dir, src, out, scale, nfields, accumulate);
+  if (c->g.n2 <= 65535) {
+    const int bx = c->g.n1 >= 128 ? 128 : (c->g.n1 >= 64 ? 64 : 32);
+    const dim3 grid((c->g.n1 + bx - 1) / bx, c->g.n2, std::min(c->g.n3 * nfields, 65535));
+    if (dir == 0) k_band_T_grid<0><<<grid, bx, 0, c->stream>>>(t, c->g, src, out, scale, nfields, accumulate);
+    else if (dir == 1) k_band_T_grid<1><<<grid, bx, 0, c->stream>>>(t, c->g, src, out, scale, nfields, accumulate);
+    else k_band_T_grid<2><<<grid, bx, 0, c->stream>>>(t, c->g, src, out, scale, nfields, accumulate);
+  } else {
+    k_band_T<<<(int)std::min<long long>(nblocks(M), 148LL * 64), kThreads, 0, c->stream>>>(
+        t, c->g, dir, src, out, scale, nfields, accumulate);
+  }
   CRUNA_LAUNCH_CHECK(c);
 }
 
