@@ -1,0 +1,43 @@
+"""The measurement scripts behind the profile summaries run end to end on small sizes: run_case
+(direct and adjoint timing, kernel-family profile), tgv_study (FP64 against FP32 stencils with
+kinetic-energy and enstrophy histories), enstrophy_study (enstrophy gradient against central
+differences) and mlp_bench (closure MLP kernels)."""
+import argparse
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_run_case_times_and_profiles():
+    from public_b200 import run_case
+    base = dict(case="mixing_layer", n=[32, 48, 16], steps=3, warmup=1, adjoint=True, no_graphs=False, json=None)
+    out = run_case.run(argparse.Namespace(**base, profile=False))
+    assert out["rhs_path"] == "generic" and out["direct_ms_per_step"] > 0 and out["adjoint_ms_per_step"] > 0
+    out = run_case.run(argparse.Namespace(**dict(base, adjoint=False), profile=True))
+    assert abs(sum(v["share"] for v in out["kernels"].values()) - 1.0) < 1e-3
+    out = run_case.run(argparse.Namespace(**dict(base, case="taylor_green", n=[24], adjoint=False), profile=False))
+    assert out["rhs_path"] == "fused"
+
+
+def test_tgv_study_small():
+    from public_b200 import tgv_study
+    out = tgv_study.run(argparse.Namespace(n=24, steps=20, every=10))
+    assert len(out["fp64"]["history"]["step"]) == 3
+    assert max(out["fp32_vs_fp64_rel_l2"]) < 1e-5
+    assert out["kinetic_energy_max_rel_diff"] < 1e-6 and out["enstrophy_max_rel_diff"] < 1e-5
+
+
+def test_enstrophy_study_small():
+    from public_b200 import enstrophy_study
+    out = enstrophy_study.run(argparse.Namespace(n=24, steps=6, nsnap=2, ndir=1, eps=1e-4, precision="fp64"))
+    assert out["J"] == pytest.approx(out["J_objective_value"], rel=1e-12)
+    assert out["directions"][0]["rel_err"] < 1e-2
+
+
+def test_mlp_bench_small():
+    from public_b200 import mlp_bench
+    out = mlp_bench.run(argparse.Namespace(n=131072, train_n=16384, batch=1024, steps=5))
+    for key in ("forward", "gradient", "train_step"):
+        assert np.isfinite(out[key]["ms"]) and out[key]["ms"] > 0
