@@ -462,7 +462,8 @@ int cruna_init(const cruna_config *cfg, const double *bc_table, int nbc, cruna_c
     void *fl = nullptr;
     CRUNA_CUDA_CHECK(cudaMalloc(&fl, sizeof(int) * 4));
     c->allocations.push_back(fl);
-    c->flag = static_cast<int *>(fl);
+    c->flag = static_cast<int *>(fl);  // [0] state check, [1] a kernel's bounded wait ran out
+    CRUNA_CUDA_CHECK(cudaMemsetAsync(fl, 0, sizeof(int) * 4, c->stream));
     c->fused_ok = fused_supported(c);
     c->filter_fused_ok = filter_fused_supported(c);
     CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
@@ -517,6 +518,12 @@ void cruna_free(cruna_ctx *c) {
 int cruna_sync(cruna_ctx *c) {
   return guarded(c, [&]() -> int {
     CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+    int waited = 0;
+    CRUNA_CUDA_CHECK(cudaMemcpy(&waited, c->flag + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    if (waited) {
+      CRUNA_CUDA_CHECK(cudaMemset(c->flag + 1, 0, sizeof(int)));
+      fail(c, CRUNA_ERR_CUDA, "a kernel's bounded wait for its shared-memory copies ran out");
+    }
     return CRUNA_OK;
   });
 }

@@ -7,8 +7,12 @@
 // pass 1 filters each plane in x and then y on 32 x 32 tiles with 5-wide halos (corners included,
 // so the y filter sees x-filtered halo rows); pass 2 filters in z with a per-thread register queue
 // of 11 planes.  Each pass reads and writes the state once.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "cruna_internal.cuh"
 #include "fused_common.cuh"
+#include "tcgen05.cuh"
 
 namespace cruna {
 
@@ -128,6 +132,98 @@ __global__ void __launch_bounds__(FTHR) k_filter_z(const __grid_constant__ Filte
   }
 }
 
+// pass 2 with the loads in shared memory: the block's 32 x 8 tile of one variable streams plane by
+// plane into a ring of ZD shared slots by TMA (cp.async.bulk.tensor, issued ZD planes ahead by one
+// thread, completion counted on a per-slot mbarrier), so no registers hold loads in flight.  Plane
+// coordinates wrap periodically on the host side of each copy.  Every wait is bounded: when one runs
+// out the block records it in err, waits (bounded) for its copies in flight and returns.
+constexpr int ZD = 8;                          // planes in flight
+constexpr long long kTmaWaitLimit = 1LL << 22;
+
+__device__ __forceinline__ void tma_plane(const CUtensorMap *tm, double *dst, uint64_t *bar, int x, int y, int z,
+                                          int v) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_addr(bar)), "r"(32 * 8 * 8)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(tc::smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(v), "r"(tc::smem_addr(bar))
+      : "memory");
+}
+
+__global__ void __launch_bounds__(FTHR) k_filter_z_tma(const __grid_constant__ CUtensorMap tm,
+                                                      const __grid_constant__ FilterArgs a, int *err) {
+  constexpr int NQ = 2 * FR + 1;
+  __shared__ __align__(128) double ring[ZD][FTHR];
+  __shared__ __align__(8) uint64_t full[ZD];
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 8;
+  const int i = i0 + tid % 32, j = j0 + tid / 32;
+  const int v = blockIdx.z % 5, chunk = blockIdx.z / 5;
+  const int k0 = chunk * a.kc, k1 = min(k0 + a.kc, a.g.n3);
+  const int n3 = a.n[2];
+  const int kfirst = k0 - FR, nplanes = k1 - k0 + 2 * FR;  // planes kfirst .. kfirst + nplanes - 1
+  const long long n12 = (long long)a.g.n1 * a.g.n2;
+  double *out = a.out + (long long)v * a.g.N + i + (long long)a.g.n1 * j;
+  if (tid == 0) {
+    for (int s = 0; s < ZD; ++s) tc::mbar_init(&full[s], 1);
+    for (int idx = 0; idx < min(ZD, nplanes); ++idx)
+      tma_plane(&tm, ring[idx], &full[idx], i0, j0, wrapi(kfirst + idx, n3), v);
+  }
+  __syncthreads();
+  double q[NQ];
+  int ok = 1, issued = min(ZD, nplanes);
+  for (int idx = 0; idx < nplanes; ++idx) {
+    const int s = idx % ZD;
+    ok = __syncthreads_and(ok && tc::mbar_wait(&full[s], (uint32_t)((idx / ZD) & 1), kTmaWaitLimit));
+    if (!ok) break;
+    // every thread is past the read of plane idx - 1: its slot takes plane idx - 1 + ZD
+    if (tid == 0 && idx >= 1 && idx - 1 + ZD < nplanes) {
+      tc::fence_async_smem();
+      const int r = idx - 1 + ZD;
+      tma_plane(&tm, ring[r % ZD], &full[r % ZD], i0, j0, wrapi(kfirst + r, n3), v);
+      issued = r + 1;
+    }
+#pragma unroll
+    for (int m = 0; m < NQ - 1; ++m) q[m] = q[m + 1];
+    q[NQ - 1] = ring[s][tid];
+    if (idx >= 2 * FR && i < a.g.n1 && j < a.g.n2) out[n12 * (kfirst + idx - FR)] = filt(a, q + FR, 1);
+  }
+  if (!ok) {
+    if (tid == 0) {
+      atomicExch(err, 1);
+      // the copies possibly still in flight are the last ZD issued (one per slot, its latest phase)
+      for (int r = max(0, issued - ZD); r < issued; ++r)
+        tc::mbar_wait(&full[r % ZD], (uint32_t)((r / ZD) & 1), kTmaWaitLimit);
+    }
+    __syncthreads();
+  }
+}
+
+// 4-D tensor map (n1, n2, n3, 5) of a Fortran-ordered FP64 state with a 32 x 8 x 1 x 1 box; false
+// when the layout does not meet TMA's rules (n1 even, so every row stride is a multiple of 16 bytes)
+bool state_tensor_map(const cruna_ctx *c, const double *state, CUtensorMap *tm) {
+  if (c->g.n1 % 2 != 0 || (reinterpret_cast<uintptr_t>(state) & 15) != 0) return false;
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      cudaGetLastError();
+      return false;
+    }
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[4] = {(cuuint64_t)c->g.n1, (cuuint64_t)c->g.n2, (cuuint64_t)c->g.n3, 5};
+  const cuuint64_t strides[3] = {(cuuint64_t)c->g.n1 * 8, (cuuint64_t)c->g.n1 * c->g.n2 * 8,
+                                 (cuuint64_t)c->g.N * 8};
+  const cuuint32_t box[4] = {32, 8, 1, 1}, elem[4] = {1, 1, 1, 1};
+  return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double *>(state), dims, strides, box, elem,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 // filters usable by the fused passes: the explicit periodic o10 filter or none, in every direction
@@ -190,7 +286,11 @@ void filter3_fused(cruna_ctx *c, const double *in, double *out, const int on_in[
     a.kc = (n3 + nz - 1) / nz;
     nz = (n3 + a.kc - 1) / a.kc;
     ProfScope ps(c, "filter_z");
-    k_filter_z<<<dim3(zx, zy, 5 * nz), FTHR, 0, c->stream>>>(a);
+    CUtensorMap tm;
+    if (state_tensor_map(c, src, &tm))
+      k_filter_z_tma<<<dim3(zx, zy, 5 * nz), FTHR, 0, c->stream>>>(tm, a, c->flag + 1);
+    else
+      k_filter_z<<<dim3(zx, zy, 5 * nz), FTHR, 0, c->stream>>>(a);
     CRUNA_LAUNCH_CHECK(c);
   }
 }
