@@ -115,6 +115,7 @@ _SIGNATURES = {
     "cruna_profile_enable": (_I, [_P, _I]),
     "cruna_profile_report": (_I, [_P, C.c_char_p, _I]),
     "cruna_set_graphs": (_I, [_P, _I]),
+    "cruna_set_snapshot_memory": (_I, [_P, _I]),
     "cruna_set_closure_normalisation": (_I, [_P, _I]),
     "cruna_diagnostics": (_I, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "cruna_diagnostics_dev": (_I, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -564,6 +565,10 @@ class Cruna:
         ke, en = C.c_double(), C.c_double()
         self._check(self.lib.cruna_diagnostics_dev(self.h, C.c_void_p(q_ptr), C.byref(ke), C.byref(en)))
         return ke.value, en.value
+
+    def set_snapshot_memory(self, host: bool):
+        """Keep cruna_gradient's snapshots in pinned host memory (True) or in HBM (False, default)."""
+        self._check(self.lib.cruna_set_snapshot_memory(self.h, 1 if host else 0))
 
     def set_graphs(self, on: bool = True):
         """Record repeating loop steps as CUDA graphs inside run / gradient calls (default on)."""

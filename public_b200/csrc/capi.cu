@@ -123,9 +123,23 @@ void stage_out(cruna_ctx *c, double *host, const double *dev, int nfields) {
   CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
 }
 
+// the reference state buffer (zeros until cruna_set_reference)
+void ensure_reference(cruna_ctx *c) {
+  if (c->qref) return;
+  c->qref = dalloc(c, (size_t)N5(c));
+  CRUNA_CUDA_CHECK(cudaMemsetAsync(c->qref, 0, sizeof(double) * N5(c), c->stream));
+}
+
+// the RHS buffer st[0]: the generic path's RHS and the fused path's RHS before RHS boundary conditions
+double *rhs_buffer(cruna_ctx *c) {
+  if (!c->st[0]) c->st[0] = dalloc(c, (size_t)N5(c));
+  return c->st[0];
+}
+
 // time_stepper_direct (rk_o4_e.f90:17-58): q1 may alias q0
 void step_direct(cruna_ctx *c, const double *q0, double *q1) {
-  double *k = c->st[0], *acc = c->st[1], *qa = c->st[2], *qb = c->st[3], *qbc = c->st[4];
+  double *k = (use_fused(c) && !c->has_rhs_bc) ? nullptr : rhs_buffer(c);
+  double *acc = c->st[1], *qa = c->st[2], *qb = c->st[3], *qbc = c->st[4];
   const double dt = c->cfg.dt;
   if (use_fused(c)) {
     halo(c, q0, 5);
@@ -163,7 +177,8 @@ void step_direct(cruna_ctx *c, const double *q0, double *q1) {
 
 // time_stepper_adjoint (rk_o4_e.f90:62-105): dt -> -dt, q0 frozen; qs1 may alias qs0
 void step_adjoint(cruna_ctx *c, const double *qs0, const double *q0, const double *g, double *qs1) {
-  double *k = c->st[0], *acc = c->st[1], *qa = c->st[2], *qb = c->st[3], *qbc = c->st[4];
+  double *k = (use_fused(c) && !c->has_rhs_bc) ? nullptr : rhs_buffer(c);
+  double *acc = c->st[1], *qa = c->st[2], *qb = c->st[3], *qbc = c->st[4];
   const double dt = -c->cfg.dt;
   halo(c, q0, 5);
   if (use_fused(c)) {
@@ -455,10 +470,14 @@ int cruna_init(const cruna_config *cfg, const double *bc_table, int nbc, cruna_c
       c->sponge.amp = cfg->sponge_amplitude;
     }
     if (c->kvec) build_kvector(c);
-    // reference state defaults to zero until cruna_set_reference
-    c->qref = dalloc(c, (size_t)N5(c));
-    CRUNA_CUDA_CHECK(cudaMemsetAsync(c->qref, 0, sizeof(double) * N5(c), c->stream));
-    for (int i = 0; i < 6; ++i) c->st[i] = dalloc(c, (size_t)N5(c));
+    // reference state (zero until cruna_set_reference), only where a boundary type reads it
+    bool needs_ref = false;
+    for (const BCRow &r : c->bc) needs_ref = needs_ref || (r.type >= 201 && r.type <= 206) || r.type >= 400;
+    if (needs_ref) ensure_reference(c);
+    // stage buffers: acc, two stage inputs and the step output always; the RHS buffer st[0] and the
+    // BC copy st[4] on first use (the fused passes without RHS boundary conditions need neither)
+    for (int i : {1, 2, 3, 5}) c->st[i] = dalloc(c, (size_t)N5(c));
+    if (c->has_q_bc) c->st[4] = dalloc(c, (size_t)N5(c));
     void *fl = nullptr;
     CRUNA_CUDA_CHECK(cudaMalloc(&fl, sizeof(int) * 4));
     c->allocations.push_back(fl);
@@ -549,6 +568,7 @@ int64_t cruna_kernel_launches(const cruna_ctx *c) { return c ? c->launches : -1;
 int cruna_set_reference_dev(cruna_ctx *c, const double *qref) {
   return guarded(c, [&]() -> int {
     if (!qref) fail(c, CRUNA_ERR_ARG, "qref is null");
+    ensure_reference(c);
     copy_state(c, c->qref, qref, 5);
     return CRUNA_OK;
   });
@@ -557,6 +577,7 @@ int cruna_set_reference_dev(cruna_ctx *c, const double *qref) {
 int cruna_set_reference(cruna_ctx *c, const double *qref) {
   return guarded(c, [&]() -> int {
     if (!qref) fail(c, CRUNA_ERR_ARG, "qref is null");
+    ensure_reference(c);
     CRUNA_CUDA_CHECK(cudaMemcpyAsync(c->qref, qref, sizeof(double) * N5(c), cudaMemcpyHostToDevice, c->stream));
     CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
     return CRUNA_OK;
@@ -1193,6 +1214,13 @@ int cruna_set_halo_exchange(cruna_ctx *c, int (*fn)(void *, double *, int, void 
       fail(c, CRUNA_ERR_UNSUPPORTED, "z slabs need a periodic z scheme and no boundary table");
     c->halo_fn = fn;
     c->halo_user = user;
+    return CRUNA_OK;
+  });
+}
+
+int cruna_set_snapshot_memory(cruna_ctx *c, int host) {
+  return guarded(c, [&]() -> int {
+    c->snapshot_host = host != 0;
     return CRUNA_OK;
   });
 }

@@ -172,8 +172,8 @@ struct cruna_ctx {
   double *cl_force = nullptr;      // forcing + closure stress divergence (5N)
   double *cl_tau = nullptr;        // model stresses (6N) and their derivatives (9N)
   float *cl_x = nullptr, *cl_y = nullptr;  // features (12N) and outputs (6N), point-major
-  double *ens_ws = nullptr;        // enstrophy objective / diagnostics workspace (8N)
   double *diag = nullptr;          // diagnostics reduction scratch (partials + 2 results)
+  bool snapshot_host = false;      // gradient snapshots in pinned host memory instead of HBM
   // step graphs (step_graph.cu): the cache of the current run call, or null outside one
   bool graphs_enabled = true;
   cruna::StepGraphs *graphs = nullptr;

@@ -246,7 +246,7 @@ bool filter_fused_supported(const cruna_ctx *c) {
 }
 
 // out = filter_i3(filter_i2(filter_i1(in))) restricted to the directions with on[d] != 0; in != out.
-// Uses the stage buffer st[0] as the intermediate between the two passes.
+// Uses the stage buffer st[2] (free after a time step) as the intermediate between the two passes.
 void filter3_fused(cruna_ctx *c, const double *in, double *out, const int on_in[3]) {
   FilterArgs a;
   a.g = c->g;
@@ -265,7 +265,7 @@ void filter3_fused(cruna_ctx *c, const double *in, double *out, const int on_in[
       for (int m = 0; m <= FR; ++m) a.c[m] = c->fop[d].c[m];
       a.blend = c->fop[d].blend;
     }
-  double *tmp = c->st[0];
+  double *tmp = c->st[2];
   const double *src = in;
   a.kc = 1;
   if (a.on[0] || a.on[1]) {

@@ -201,11 +201,11 @@ double cell_volume(const cruna_ctx *c) {
 }
 
 // Z = sum dV |curl u|^2 / 2 with the context's derivative operators (h = dx) into J (scaled by 1,
-// accumulated or not); lam (optional) = dZ/dq through the transposed operators.  Workspace: 8 fields.
+// accumulated or not); lam (optional) = dZ/dq through the transposed operators.  Workspace: the stage
+// buffers st[2] (u, a temporary, the transposes' scratch) and st[3] (omega), free between steps.
 void enstrophy_objective(cruna_ctx *c, const double *q, double *lam, double *partial, double *J, int accumulate) {
   const long long N = c->g.N;
-  if (!c->ens_ws) c->ens_ws = dalloc(c, (size_t)N * 8);
-  double *u = c->ens_ws, *w = u + 3 * N, *t = u + 6 * N, *scr = u + 7 * N;
+  double *u = c->st[2], *t = u + 3 * N, *scr = u + 4 * N, *w = c->st[3];
   const int blocks = (int)std::min<long long>((N + 255) / 256, 148LL * 16);
   k_velocity<<<blocks, 256, 0, c->stream>>>(N, q, u);
   CRUNA_LAUNCH_CHECK(c);
@@ -286,7 +286,17 @@ struct GradientRun {
       }
     throw std::runtime_error("checkpoint schedule ran out of snapshots");
   }
-  void copy(double *dst, const double *src) { copy_state(c, dst, src, 5); }
+  bool host_slots = false;         // snapshots in pinned host memory (cruna_set_snapshot_memory)
+  void copy(double *dst, const double *src) {
+    if (dst == src) return;
+    CRUNA_CUDA_CHECK(cudaMemcpyAsync(dst, src, sizeof(double) * c->g.N * 5, cudaMemcpyDefault, c->stream));
+  }
+  // the state held by snapshot slot sm, where the kernels can read it (host slots go through work)
+  const double *at_snapshot(int sm) {
+    if (!host_slots) return slots[sm];
+    copy(work, slots[sm]);
+    return work;
+  }
   void advance(int a, int b) {
     for (int nt = a + 1; nt <= b; ++nt) {
       direct_step(c, work, nt);
@@ -376,7 +386,7 @@ struct GradientRun {
     const int sm = take(m);
     copy(slots[sm], work);
     rev(m, b, s - 1);
-    adjoint(m, slots[sm]);
+    adjoint(m, at_snapshot(sm));
     slot_step[sm] = -1;
     rev(a, m - 1, s);
   }
@@ -386,8 +396,20 @@ struct GradientRun {
 void direct_loop_step(cruna_ctx *c, double *q, int nt);
 void adjoint_loop_step(cruna_ctx *c, double *qs, const double *q0, const double *g, int nt);
 
+// pinned host snapshot buffers, released once the stream has finished with them
+struct PinnedBuffers {
+  cudaStream_t stream;
+  std::vector<void *> p;
+  ~PinnedBuffers() {
+    if (p.empty()) return;
+    cudaStreamSynchronize(stream);
+    for (void *x : p) cudaFreeHost(x);
+  }
+};
+
 long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
                         double *J_dev, double *grad_f, double *grad_q0, std::vector<void *> &scratch) {
+  PinnedBuffers pinned{c->stream, {}};
   GraphScope graphs(c);
   GradientRun g;
   g.c = c;
@@ -406,27 +428,38 @@ long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, c
     scratch.push_back(p);
     return static_cast<double *>(p);
   };
+  const bool plane = obj->kind == CRUNA_OBJ_PLANE_P2;
   g.work = alloc(bytes);
   g.slots.resize(g.S + 1);
   g.slot_step.assign(g.S + 1, -1);
-  for (int i = 0; i <= g.S; ++i) g.slots[i] = alloc(bytes);
+  g.host_slots = c->snapshot_host;
+  for (int i = 0; i <= g.S; ++i) {
+    if (g.host_slots) {
+      void *p = nullptr;
+      CRUNA_CUDA_CHECK(cudaMallocHost(&p, bytes));
+      pinned.p.push_back(p);
+      g.slots[i] = static_cast<double *>(p);
+    } else {
+      g.slots[i] = alloc(bytes);
+    }
+  }
   g.qs = alloc(bytes);
-  g.gsrc = alloc(bytes);
+  g.gsrc = plane ? alloc(bytes) : nullptr;  // the plane objective's adjoint source
   g.partial = alloc(sizeof(double) * (RG + 1));
   g.J = J_dev;
   g.gf = grad_f;
   CRUNA_CUDA_CHECK(cudaMemsetAsync(g.qs, 0, bytes, c->stream));
-  CRUNA_CUDA_CHECK(cudaMemsetAsync(g.gsrc, 0, bytes, c->stream));
+  if (plane) CRUNA_CUDA_CHECK(cudaMemsetAsync(g.gsrc, 0, bytes, c->stream));
   CRUNA_CUDA_CHECK(cudaMemsetAsync(J_dev, 0, sizeof(double), c->stream));
   g.direct_step = direct_loop_step;
   g.adjoint_step = adjoint_loop_step;
   g.slot_step[0] = 0;
-  copy_state(c, g.slots[0], q0, 5);
+  g.copy(g.slots[0], q0);  // q0 is not read after this copy (grad_q0 may alias it)
   if (g.discrete) {
     g.qN = alloc(bytes);
     if (grad_f) CRUNA_CUDA_CHECK(cudaMemsetAsync(grad_f, 0, bytes, c->stream));
     g.rev(0, span, g.S);
-    g.adjoint(0, g.slots[0]);
+    g.adjoint(0, g.at_snapshot(0));
   } else {
     g.rev(0, nsteps, g.S);
   }
@@ -446,11 +479,11 @@ double objective_direct_impl(cruna_ctx *c, const double *q0, int nsteps, const c
     return static_cast<double *>(p);
   };
   const size_t bytes = sizeof(double) * (size_t)c->g.N * 5;
-  double *work = alloc(bytes), *gsrc = alloc(bytes), *partial = alloc(sizeof(double) * (RG + 1)),
-         *J = alloc(sizeof(double));
+  const bool plane = obj->kind == CRUNA_OBJ_PLANE_P2;
+  double *work = alloc(bytes), *gsrc = plane ? alloc(bytes) : nullptr,
+         *partial = alloc(sizeof(double) * (RG + 1)), *J = alloc(sizeof(double));
   CRUNA_CUDA_CHECK(cudaMemsetAsync(J, 0, sizeof(double), c->stream));
   copy_state(c, work, q0, 5);
-  const bool plane = obj->kind == CRUNA_OBJ_PLANE_P2;
   const int nd = obj->normal - 1;
   double w = 1.0;
   for (int d = 0; d < 3; ++d)

@@ -77,3 +77,26 @@ def test_enstrophy_gradient_fp32_stencils_close_to_fp64():
     (J64, gf64, gq64, _), (J32, gf32, gq32, _) = out["fp64"], out["fp32"]
     assert abs(J32 - J64) < 1e-6 * abs(J64)
     assert np.linalg.norm(gq32 - gq64) < 1e-5 * np.linalg.norm(gq64)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_host_snapshots_and_aliased_gradient_match_hbm(mode):
+    """Snapshots in pinned host memory give the same bits as HBM snapshots, and cruna_gradient_dev
+    may write dJ/dq0 over q0 itself."""
+    s, q = cases.taylor_green(n=16, seed=1)
+    s["mu0"] = 0.02
+    out = {}
+    for host in (False, True):
+        with Cruna(Settings.from_dict(s), force=np.zeros_like(q)) as c:
+            c.set_adjoint_mode(mode)
+            c.set_snapshot_memory(host)
+            out[host] = c.gradient(q, 7, 3, c.objective("enstrophy"))
+            qt = torch.from_numpy(np.ascontiguousarray(q.ravel(order="F"))).cuda()
+            torch.cuda.synchronize()
+            J, steps = c.gradient_dev(qt.data_ptr(), 7, 3, c.objective("enstrophy"), None, qt.data_ptr())
+            c.sync()
+            assert J == out[host][0] and steps == out[host][3]
+            assert np.array_equal(qt.cpu().numpy().reshape(q.shape, order="F"), out[host][2])
+    (J0, gf0, gq0, n0), (J1, gf1, gq1, n1) = out[False], out[True]
+    assert J0 == J1 and n0 == n1
+    assert np.array_equal(gq0, gq1) and np.array_equal(gf0, gf1)

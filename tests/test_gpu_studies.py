@@ -31,9 +31,12 @@ def test_tgv_study_small():
 
 def test_enstrophy_study_small():
     from public_b200 import enstrophy_study
-    out = enstrophy_study.run(argparse.Namespace(n=24, steps=6, nsnap=2, ndir=1, eps=1e-4, precision="fp64"))
+    base = dict(n=24, steps=6, nsnap=2, ndir=1, eps=1e-4, precision="fp64")
+    out = enstrophy_study.run(argparse.Namespace(**base, host_snapshots=False))
     assert out["J"] == pytest.approx(out["J_objective_value"], rel=1e-12)
     assert out["directions"][0]["rel_err"] < 1e-2
+    host = enstrophy_study.run(argparse.Namespace(**base, host_snapshots=True))
+    assert host["J"] == out["J"] and host["directions"][0]["adjoint"] == out["directions"][0]["adjoint"]
 
 
 def test_mlp_bench_small():
