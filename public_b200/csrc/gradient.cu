@@ -287,14 +287,55 @@ struct GradientRun {
     throw std::runtime_error("checkpoint schedule ran out of snapshots");
   }
   bool host_slots = false;         // snapshots in pinned host memory (cruna_set_snapshot_memory)
+  // Host slots, when HBM has room for one more state: hcache holds the last slot stored or loaded.
+  // A store copies work into it and drains it to the host on a copy stream while the direct steps
+  // go on; a load of the cached slot (the restart right after a store, each restart of a leaf) is a
+  // device copy.  The cache is overwritten only after its pending drain (d2h_done) has finished.
+  double *hcache = nullptr;
+  int hcache_slot = -1;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t cache_ready = nullptr, d2h_done = nullptr;
+  ~GradientRun() {
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
+    if (cache_ready) cudaEventDestroy(cache_ready);
+    if (d2h_done) cudaEventDestroy(d2h_done);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+  }
+  void enable_cache(double *buf) {
+    CRUNA_CUDA_CHECK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+    CRUNA_CUDA_CHECK(cudaEventCreateWithFlags(&cache_ready, cudaEventDisableTiming));
+    CRUNA_CUDA_CHECK(cudaEventCreateWithFlags(&d2h_done, cudaEventDisableTiming));
+    hcache = buf;
+  }
   void copy(double *dst, const double *src) {
     if (dst == src) return;
     CRUNA_CUDA_CHECK(cudaMemcpyAsync(dst, src, sizeof(double) * c->g.N * 5, cudaMemcpyDefault, c->stream));
   }
+  void fill_cache(const double *src, int s) {
+    CRUNA_CUDA_CHECK(cudaStreamWaitEvent(c->stream, d2h_done, 0));
+    copy(hcache, src);
+    hcache_slot = s;
+  }
+  // dst <- snapshot slot s
+  void load(double *dst, int s) {
+    if (!hcache) return copy(dst, slots[s]);
+    if (hcache_slot != s) fill_cache(slots[s], s);
+    copy(dst, hcache);
+  }
+  // snapshot slot s <- work
+  void store(int s) {
+    if (!hcache) return copy(slots[s], work);
+    fill_cache(work, s);
+    CRUNA_CUDA_CHECK(cudaEventRecord(cache_ready, c->stream));
+    CRUNA_CUDA_CHECK(cudaStreamWaitEvent(copy_stream, cache_ready, 0));
+    CRUNA_CUDA_CHECK(cudaMemcpyAsync(slots[s], hcache, sizeof(double) * c->g.N * 5, cudaMemcpyDeviceToHost,
+                                     copy_stream));
+    CRUNA_CUDA_CHECK(cudaEventRecord(d2h_done, copy_stream));
+  }
   // the state held by snapshot slot sm, where the kernels can read it (host slots go through work)
   const double *at_snapshot(int sm) {
     if (!host_slots) return slots[sm];
-    copy(work, slots[sm]);
+    load(work, sm);
     return work;
   }
   void advance(int a, int b) {
@@ -373,7 +414,7 @@ struct GradientRun {
     const int sa = slot_of(a);
     if (s == 0) {
       for (int nt = b; nt > a; --nt) {
-        copy(work, slots[sa]);
+        load(work, sa);
         advance(a, nt);
         adjoint(nt, work);
       }
@@ -381,10 +422,10 @@ struct GradientRun {
     }
     const int k = kbest[(size_t)n * (S + 1) + s];
     const int m = a + k;
-    copy(work, slots[sa]);
+    load(work, sa);
     advance(a, m);
     const int sm = take(m);
-    copy(slots[sm], work);
+    store(sm);
     rev(m, b, s - 1);
     adjoint(m, at_snapshot(sm));
     slot_step[sm] = -1;
@@ -429,7 +470,8 @@ long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, c
     return static_cast<double *>(p);
   };
   const bool plane = obj->kind == CRUNA_OBJ_PLANE_P2;
-  g.work = alloc(bytes);
+  double *work = alloc(bytes);
+  g.work = work;
   g.slots.resize(g.S + 1);
   g.slot_step.assign(g.S + 1, -1);
   g.host_slots = c->snapshot_host;
@@ -453,10 +495,21 @@ long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, c
   CRUNA_CUDA_CHECK(cudaMemsetAsync(J_dev, 0, sizeof(double), c->stream));
   g.direct_step = direct_loop_step;
   g.adjoint_step = adjoint_loop_step;
+  if (g.discrete) g.qN = alloc(bytes);
+  if (g.host_slots && span > 0) {  // optional, last: without room for it every restart crosses PCIe
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) == cudaSuccess) {
+      scratch.push_back(p);
+      g.enable_cache(static_cast<double *>(p));
+    } else {
+      (void)cudaGetLastError();
+    }
+  }
   g.slot_step[0] = 0;
-  g.copy(g.slots[0], q0);  // q0 is not read after this copy (grad_q0 may alias it)
+  g.work = const_cast<double *>(q0);  // q0 is not read after this store (grad_q0 may alias it)
+  g.store(0);
+  g.work = work;
   if (g.discrete) {
-    g.qN = alloc(bytes);
     if (grad_f) CRUNA_CUDA_CHECK(cudaMemsetAsync(grad_f, 0, bytes, c->stream));
     g.rev(0, span, g.S);
     g.adjoint(0, g.at_snapshot(0));

@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import sys
 import time
 
 import numpy as np
@@ -46,6 +47,7 @@ def run(args) -> dict:
         J, adv = c.gradient_dev(q.data_ptr(), args.steps, args.nsnap, obj, None, q.data_ptr())  # q <- dJ/dq0
         c.sync()
         out.update(J=J, gradient_seconds=time.time() - t0, direct_steps=adv)
+        print(json.dumps(out), file=sys.stderr, flush=True)
         gq = q
         q = torch.from_numpy(np.ascontiguousarray(q0.ravel(order="F"))).to(dev)
         torch.cuda.synchronize()
@@ -57,6 +59,7 @@ def run(args) -> dict:
         c.sync()
         out["J_objective_value"] = J0
         out["ms_per_direct_step_with_objective"] = e0.elapsed_time(e1) / args.steps
+        print(json.dumps(out), file=sys.stderr, flush=True)
         gen = torch.Generator(device=dev)
         gen.manual_seed(5)
         dirs = []
@@ -64,7 +67,8 @@ def run(args) -> dict:
             d = torch.zeros_like(q)
             for v in range(3):
                 d[(1 + v) * N:(2 + v) * N] = torch.randn(N, generator=gen, device=dev, dtype=torch.float64) * q[:N] * u0
-            dirs.append((d, float(torch.dot(gq, d).item())))
+            dot = sum(float(torch.dot(a, b).item()) for a, b in zip(gq.split(1 << 28), d.split(1 << 28)))
+            dirs.append((d, dot))  # cuBLAS dot takes at most 2^31 - 1 elements: sum it in chunks
             if k == 0 and args.ndir == 1:
                 break
         del gq
