@@ -17,6 +17,13 @@
 --normalised trains and runs the scale-free closure (``cruna_set_closure_normalisation``): features
 grad u / |grad u| and |grad u| delta, targets tau / (rho (|grad u| delta)^2).
 
+4. For each --gradient-steps H (a multiple of --every): the gradient of the kinetic energy after H
+   fine steps with respect to the initial fine state (continuous adjoint, binomial checkpointing),
+   summed over each filter block -- the gradient with respect to the coarse initial state of a
+   perturbation constant over the block -- against the coarse gradients over the same time
+   (H / every * 2 coarse steps) of the plain and the closure-augmented coarse solve: cosine
+   similarity over the momentum components (the initial velocity) and over the whole state.
+
 Prints one JSON object.  Data are synthetic (seeded spectrum, no dataset).
 """
 from __future__ import annotations
@@ -133,6 +140,7 @@ def run(args) -> dict:
 
         ke_plain, ms_plain = coarse_run(False)
         ke_model, ms_model = coarse_run(True)
+        grad = [gradient_comparison(args, H, fine, coarse, mlp, q0, qc0, delta) for H in args.gradient_steps]
         mlp.close()
     ke_dns = np.array(ke_dns)
 
@@ -154,8 +162,47 @@ def run(args) -> dict:
         "gpu_ms_dns": dns_ms, "gpu_ms_coarse_plain": ms_plain, "gpu_ms_coarse_closure": ms_model,
         "speedup_closure_vs_dns": dns_ms / ms_model if ms_model > 0 else None,
         "times": [float(t) for t in t_dns], "ke_dns": ke_dns.tolist(), "ke_plain": ke_plain.tolist(),
-        "ke_closure": ke_model.tolist(),
+        "ke_closure": ke_model.tolist(), "gradient": grad,
     }
+
+
+def gradient_comparison(args, H: int, fine, coarse, mlp, q0, qc0, delta) -> dict:
+    """Cosine similarity of the block-summed fine gradient of the kinetic energy after H fine steps with
+    the plain and closure-augmented coarse gradients (momentum components and whole state)."""
+    import torch
+
+    if H % args.every:
+        raise ValueError("--gradient-steps must be a multiple of --every")
+    Hc = H // args.every * 2
+    nf, r = args.n, args.factor
+    nc = nf // r
+    dev = qc0.device
+    qf = torch.from_numpy(np.ascontiguousarray(q0.ravel(order="F"))).to(dev)
+    gf = torch.empty_like(qf)
+    torch.cuda.synchronize()
+    Jf, _ = fine.gradient_dev(qf.data_ptr(), H, args.gradient_snapshots, fine.objective("kinetic_energy"),
+                              None, gf.data_ptr())
+    fine.sync()
+    # Fortran order: flat index i + n (j + n k) + v n^3, so the view is (v, k, j, i)
+    g_block = gf.view(5, nc, r, nc, r, nc, r).sum((2, 4, 6)).reshape(-1)
+    del qf, gf
+    out = {"fine_steps": H, "coarse_steps": Hc, "J_fine": Jf}
+    Nc = nc ** 3
+    for name, model in (("plain", None), ("closure", mlp)):
+        coarse.set_closure(model, delta)
+        qq = qc0.clone()
+        gc = torch.empty_like(qq)
+        torch.cuda.synchronize()
+        Jc, _ = coarse.gradient_dev(qq.data_ptr(), Hc, args.gradient_snapshots, coarse.objective("kinetic_energy"),
+                                    None, gc.data_ptr())
+        coarse.sync()
+        coarse.set_closure(None)
+
+        def cos(a, b):
+            return float(torch.dot(a, b).item() / (torch.linalg.vector_norm(a) * torch.linalg.vector_norm(b)).item())
+
+        out[name] = {"J": Jc, "cos_momentum": cos(g_block[Nc:4 * Nc], gc[Nc:4 * Nc]), "cos_state": cos(g_block, gc)}
+    return out
 
 
 def main(argv=None):
@@ -173,6 +220,9 @@ def main(argv=None):
     ap.add_argument("--re-lambda", type=float, default=100.0)
     ap.add_argument("--normalised", action="store_true",
                     help="scale-free closure: features grad u / |grad u|, |grad u| delta; targets tau / (rho (|grad u| delta)^2)")
+    ap.add_argument("--gradient-steps", type=int, nargs="*", default=[],
+                    help="horizons (fine steps) of the fine / coarse gradient comparison")
+    ap.add_argument("--gradient-snapshots", type=int, default=64)
     ap.add_argument("--json", type=str, default=None)
     args = ap.parse_args(argv)
     out = run(args)

@@ -108,7 +108,7 @@ def test_small_closure_study_runs_end_to_end(normalised):
     import argparse
     args = argparse.Namespace(
         n=64, factor=4, steps=40, every=10, samples=8192, train_steps=60, batch=512, lr=2e-3, seed=3,
-        mach_t=0.3, re_lambda=60.0, normalised=normalised, json=None)
+        mach_t=0.3, re_lambda=60.0, normalised=normalised, json=None, gradient_steps=[20], gradient_snapshots=8)
     out = closure_study.run(args)
     assert out["samples"] >= 512
     assert out["train_loss_last"] < out["train_loss_first"]
@@ -116,6 +116,10 @@ def test_small_closure_study_runs_end_to_end(normalised):
         assert len(out[key]) == 5 and all(np.isfinite(out[key]))
     assert out["ke_decay_dns"] < 1.0
     assert out["ke_max_rel_err_plain"] < 0.2 and out["ke_max_rel_err_closure"] < 0.2
+    g = out["gradient"][0]
+    assert g["coarse_steps"] == 4 and g["J_fine"] > 0
+    for mode in ("plain", "closure"):   # over 20 fine steps the coarse gradients follow the fine one
+        assert g[mode]["cos_momentum"] > 0.8 and g[mode]["J"] > 0
 
 
 def test_normalised_closure_features_and_stage():
