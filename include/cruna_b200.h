@@ -233,7 +233,8 @@ int cruna_gradient(cruna_ctx *ctx, const double *q0, int nsteps, int nsnap, cons
                    double *grad_f, double *grad_q0, int64_t *direct_steps);
 /* Where cruna_gradient keeps its nsnap snapshots: 0 = HBM (default), 1 = pinned host memory (copied
    over PCIe when stored and restored; frees nsnap states of HBM for grids whose states fill the GPU).
-   In the _dev variant grad_q0 may alias q0: q0 is read only before the first step. */
+   Pinned slots stay allocated on the context for later gradient calls until it is freed or this is
+   set back to 0.  In the _dev variant grad_q0 may alias q0: q0 is read only before the first step. */
 int cruna_set_snapshot_memory(cruna_ctx *ctx, int host);
 int cruna_gradient_dev(cruna_ctx *ctx, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
                        double *J, double *grad_f, double *grad_q0, int64_t *direct_steps);

@@ -567,7 +567,8 @@ class Cruna:
         return ke.value, en.value
 
     def set_snapshot_memory(self, host: bool):
-        """Keep cruna_gradient's snapshots in pinned host memory (True) or in HBM (False, default)."""
+        """Keep cruna_gradient's snapshots in pinned host memory (True) or in HBM (False, default).
+        The pinned slots are kept for later gradient calls until False is set or the context closes."""
         self._check(self.lib.cruna_set_snapshot_memory(self.h, 1 if host else 0))
 
     def set_graphs(self, on: bool = True):

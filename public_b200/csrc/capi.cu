@@ -530,6 +530,7 @@ void cruna_free(cruna_ctx *c) {
   }
   for (auto e : c->prof_pool) cudaEventDestroy(e);
   for (void *p : c->allocations) cudaFree(p);
+  for (void *p : c->snap_pinned) cudaFreeHost(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1221,6 +1222,11 @@ int cruna_set_halo_exchange(cruna_ctx *c, int (*fn)(void *, double *, int, void 
 int cruna_set_snapshot_memory(cruna_ctx *c, int host) {
   return guarded(c, [&]() -> int {
     c->snapshot_host = host != 0;
+    if (!c->snapshot_host && !c->snap_pinned.empty()) {  // give the pinned host slots back
+      CRUNA_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+      for (void *p : c->snap_pinned) cudaFreeHost(p);
+      c->snap_pinned.clear();
+    }
     return CRUNA_OK;
   });
 }

@@ -174,6 +174,7 @@ struct cruna_ctx {
   float *cl_x = nullptr, *cl_y = nullptr;  // features (12N) and outputs (6N), point-major
   double *diag = nullptr;          // diagnostics reduction scratch (partials + 2 results)
   bool snapshot_host = false;      // gradient snapshots in pinned host memory instead of HBM
+  std::vector<void *> snap_pinned;  // those host slots (one state each), kept for later gradient calls
   // step graphs (step_graph.cu): the cache of the current run call, or null outside one
   bool graphs_enabled = true;
   cruna::StepGraphs *graphs = nullptr;

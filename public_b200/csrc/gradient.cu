@@ -437,20 +437,8 @@ struct GradientRun {
 void direct_loop_step(cruna_ctx *c, double *q, int nt);
 void adjoint_loop_step(cruna_ctx *c, double *qs, const double *q0, const double *g, int nt);
 
-// pinned host snapshot buffers, released once the stream has finished with them
-struct PinnedBuffers {
-  cudaStream_t stream;
-  std::vector<void *> p;
-  ~PinnedBuffers() {
-    if (p.empty()) return;
-    cudaStreamSynchronize(stream);
-    for (void *x : p) cudaFreeHost(x);
-  }
-};
-
 long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, const cruna_objective *obj,
                         double *J_dev, double *grad_f, double *grad_q0, std::vector<void *> &scratch) {
-  PinnedBuffers pinned{c->stream, {}};
   GraphScope graphs(c);
   GradientRun g;
   g.c = c;
@@ -476,11 +464,13 @@ long long gradient_impl(cruna_ctx *c, const double *q0, int nsteps, int nsnap, c
   g.slot_step.assign(g.S + 1, -1);
   g.host_slots = c->snapshot_host;
   for (int i = 0; i <= g.S; ++i) {
-    if (g.host_slots) {
-      void *p = nullptr;
-      CRUNA_CUDA_CHECK(cudaMallocHost(&p, bytes));
-      pinned.p.push_back(p);
-      g.slots[i] = static_cast<double *>(p);
+    if (g.host_slots) {  // pinning is slow (seconds per state at 768^3): the slots stay on the context
+      if ((size_t)i == c->snap_pinned.size()) {
+        void *p = nullptr;
+        CRUNA_CUDA_CHECK(cudaMallocHost(&p, bytes));
+        c->snap_pinned.push_back(p);
+      }
+      g.slots[i] = static_cast<double *>(c->snap_pinned[i]);
     } else {
       g.slots[i] = alloc(bytes);
     }

@@ -97,6 +97,9 @@ def test_host_snapshots_and_aliased_gradient_match_hbm(mode):
             c.sync()
             assert J == out[host][0] and steps == out[host][3]
             assert np.array_equal(qt.cpu().numpy().reshape(q.shape, order="F"), out[host][2])
+            if host:  # the pinned slots are reused by the second call above, then given back
+                c.set_snapshot_memory(False)
+                assert np.array_equal(c.gradient(q, 7, 3, c.objective("enstrophy"))[2], out[host][2])
     (J0, gf0, gq0, n0), (J1, gf1, gq1, n1) = out[False], out[True]
     assert J0 == J1 and n0 == n1
     assert np.array_equal(gq0, gq1) and np.array_equal(gf0, gf1)
