@@ -166,6 +166,13 @@ def run(args) -> dict:
     }
 
 
+def block_sum(g, n: int, r: int):
+    """Sums of a Fortran-flattened n^3 state (torch, 5 fields) over r^3 blocks, as the Fortran-flattened
+    (n/r)^3 state: flat index i + n (j + n k) + v n^3, so the view is (v, k, j, i)."""
+    nc = n // r
+    return g.view(5, nc, r, nc, r, nc, r).sum((2, 4, 6)).reshape(-1)
+
+
 def gradient_comparison(args, H: int, fine, coarse, mlp, q0, qc0, delta) -> dict:
     """Cosine similarity of the block-summed fine gradient of the kinetic energy after H fine steps with
     the plain and closure-augmented coarse gradients (momentum components and whole state)."""
@@ -183,8 +190,7 @@ def gradient_comparison(args, H: int, fine, coarse, mlp, q0, qc0, delta) -> dict
     Jf, _ = fine.gradient_dev(qf.data_ptr(), H, args.gradient_snapshots, fine.objective("kinetic_energy"),
                               None, gf.data_ptr())
     fine.sync()
-    # Fortran order: flat index i + n (j + n k) + v n^3, so the view is (v, k, j, i)
-    g_block = gf.view(5, nc, r, nc, r, nc, r).sum((2, 4, 6)).reshape(-1)
+    g_block = block_sum(gf, nf, r)
     del qf, gf
     out = {"fine_steps": H, "coarse_steps": Hc, "J_fine": Jf}
     Nc = nc ** 3
