@@ -79,3 +79,43 @@ def test_init_without_device_fails_cleanly(lib):
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(FileNotFoundError):
         cruna.load_library(tmp_path / "nope.so")
+
+
+def header_arity():
+    """Number of parameters of every prototype in the header (function-pointer parameters count once)."""
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(cruna_[a-z0-9_]+)\s*\(", src):
+        depth, i = 1, m.end()
+        while depth:
+            depth += {"(": 1, ")": -1}.get(src[i], 0)
+            i += 1
+        params, depth, n = src[m.end():i - 1], 0, 1
+        if src[i:].lstrip()[:1] != ";":
+            continue                      # a function-pointer parameter or a macro, not a prototype
+        for ch in params:
+            depth += {"(": 1, ")": -1}.get(ch, 0)
+            n += ch == "," and depth == 0
+        out[m.group(1)] = 0 if params.strip() in ("", "void") else n
+    return out
+
+
+def test_python_binding_arity_matches_header():
+    arity = header_arity()
+    assert len(arity) >= 40
+    bad = {k: (arity[k], len(cruna._SIGNATURES[k][1])) for k in arity
+           if k in cruna._SIGNATURES and len(cruna._SIGNATURES[k][1]) != arity[k]}
+    assert not bad, bad
+
+
+def test_fortran_interfaces_match_header():
+    """The iso_c_binding interfaces printed for Fortran cases bind existing entry points with the
+    header's number of arguments."""
+    doc = open(os.path.join(os.path.dirname(HEADER), os.pardir, "INTEGRATION.md")).read()
+    arity = header_arity()
+    found = re.findall(r"(?:function|subroutine)\s+(cruna_[a-z0-9_]+)\s*\(([^)]*)\)", doc)
+    assert len(found) >= 30
+    for name, args in found:
+        assert name in arity, name
+        n = len([a for a in args.replace("&", "").split(",") if a.strip()])
+        assert n == arity[name], (name, n, arity[name])
