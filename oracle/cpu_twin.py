@@ -7,7 +7,6 @@ run() advances (direct step + filters, adjoint step + filters) pairs on Fortran-
 from __future__ import annotations
 
 import ctypes as C
-import os
 import shutil
 import subprocess
 from pathlib import Path

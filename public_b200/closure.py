@@ -10,7 +10,7 @@ tau_13, tau_23.
 from __future__ import annotations
 
 import ctypes as C
-from typing import Optional, Sequence
+from typing import Sequence
 
 import numpy as np
 

@@ -13,7 +13,7 @@ use torch.distributed point-to-point (NCCL on GPUs, gloo on CPU tensors).
 from __future__ import annotations
 
 import ctypes as C
-from typing import Dict, Optional, Tuple
+from typing import Dict, Tuple
 
 import numpy as np
 
