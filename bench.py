@@ -12,7 +12,9 @@ L2, so no explicit flush is needed between iterations.
 
 --impl reference times the C + OpenMP restatement of the reference's algorithm (oracle/cruna_cpu.c,
 checked against the numpy oracle; the Fortran reference itself cannot be built on this image) on all
-host cores, one 96^3 direct+adjoint step pair per timed step.
+host cores on the same 256^3 configuration, one direct+adjoint step pair per timed step, the state
+generated once before the warm-up.  --gpus N without a launcher re-executes the script through
+torch.distributed.run with N ranks.
 """
 from __future__ import annotations
 
@@ -56,48 +58,64 @@ def load_peaks():
 # ------------------------------------------------------------------------------------------------
 # CPU legs (oracle): bounded samples of the same physics
 # ------------------------------------------------------------------------------------------------
+class CpuTwin:
+    """The C + OpenMP restatement of the oracle (oracle/cruna_cpu.c) on an n^3 Taylor-Green state of the
+    benchmark's configuration, generated once; pair() advances one direct+adjoint step pair in place."""
+
+    def __init__(self, n: int, threads: int = 0):
+        import numpy as np
+
+        from oracle import cpu_twin
+        from public_b200 import cases
+
+        self.twin = cpu_twin
+        self.n, self.threads = n, threads
+        s, q0 = cases.taylor_green(n=n, seed=0)
+        s["ai_freq"] = (1, 1, 1)
+        self.s = s
+        self.q = np.array(q0, order="F", copy=True)
+        self.qs = np.asfortranarray(1e-3 * np.ones_like(q0))
+        self.cores = threads if threads > 0 else cpu_twin.threads()
+
+    def pairs(self, k: int) -> float:
+        """Runs k step pairs; returns the wall time in seconds."""
+        t0 = time.perf_counter()
+        self.twin.run(self.s, self.q, self.qs, k, self.threads)
+        return time.perf_counter() - t0
+
+
 def cpu_sample(n: int, pairs: int, threads: int = 0):
-    """Times `pairs` direct+adjoint step pairs of the C + OpenMP restatement of the oracle
-    (oracle/cruna_cpu.c) on an n^3 Taylor-Green sample with `threads` OpenMP threads (0: all);
-    returns (point-steps/s, seconds, threads used)."""
-    import numpy as np
-
-    from oracle import cpu_twin
-    from public_b200 import cases
-
-    s, q0 = cases.taylor_green(n=n, seed=0)
-    s["ai_freq"] = (1, 1, 1)
-    q = np.array(q0, order="F", copy=True)
-    qs = np.asfortranarray(1e-3 * np.ones_like(q0))
-    cpu_twin.run(s, q, qs, 1, threads)            # warm-up (page faults, thread pool)
-    t0 = time.perf_counter()
-    cpu_twin.run(s, q, qs, pairs, threads)
-    dt = time.perf_counter() - t0
-    used = threads if threads > 0 else cpu_twin.threads()
-    return n ** 3 * pairs / dt, dt, used
+    """Times `pairs` direct+adjoint step pairs of the CPU twin on an n^3 Taylor-Green state after one
+    untimed warm-up pair (page faults, thread pool); returns (point-steps/s, seconds, threads used)."""
+    tw = CpuTwin(n, threads)
+    tw.pairs(1)
+    dt = tw.pairs(pairs)
+    return n ** 3 * pairs / dt, dt, tw.cores
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    n = args.ref_n
-    cpu_sample(n, 1)                                     # warm-up
-    vals, t0 = [], time.perf_counter()
-    for _ in range(max(1, args.steps)):
-        v, _, cores = cpu_sample(n, 1)
-        vals.append(v)
-    wall = time.perf_counter() - t0
-    value = statistics.median(vals)
+    n = args.ref_n or args.n
+    tw = CpuTwin(n)
+    for _ in range(args.warmup):                         # untimed warm-up pairs
+        tw.pairs(1)
+    steps = max(1, args.steps)
+    times = [tw.pairs(1) for _ in range(steps)]        # one step pair of the workload per timed step
+    total = sum(times)
+    value = n ** 3 * steps / total
+    sample = (f"{n}^3 Taylor-Green (the benchmark's configuration), one direct+adjoint step pair per timed "
+              f"step, C+OpenMP restatement on all host threads")
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(1, args.steps),
+        "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded Taylor-Green state)",
-        "config": {"workload": f"taylor-green {args.n}^3, o8 FD + o10 filter, RK4, direct+adjoint step",
-                   "sample": f"{n}^3 Taylor-Green, 1 direct+adjoint step pair per timed step"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{n}^3 Taylor-Green, one direct+adjoint pair per step, C+OpenMP restatement"},
+        "data": "synthetic (seeded Taylor-Green state, 1e-4 density noise)",
+        "config": {"workload": f"taylor-green {n}^3 Mach 0.1 Re 1600: o8 FD, o10 explicit filter every step, "
+                               f"RK4 direct step + continuous-adjoint RK4 step",
+                   "points": n ** 3, "sample": sample, "same_config": n == args.n},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": tw.cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "C + OpenMP restatement of the reference algorithm in the reference's call structure "
                 "(the Fortran/MPI/HDF5 reference cannot be built on this image)",
@@ -181,10 +199,12 @@ def run_ours(args):
     # CPU baseline first (spawned processes, before heavy GPU work), rank 0 at N=1 only
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, wall, cores = cpu_sample(args.ref_n, 6)
+        n_cpu = args.ref_n or args.n
+        v, wall, cores = cpu_sample(n_cpu, args.cpu_pairs)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{args.ref_n}^3 Taylor-Green, 6 direct+adjoint step pairs, C+OpenMP restatement "
-                         f"of the oracle on all host threads", "seconds": round(wall, 2)}
+               "sample": f"{n_cpu}^3 Taylor-Green, {args.cpu_pairs} direct+adjoint step pairs after one warm-up "
+                         f"pair, C+OpenMP restatement of the oracle on all host threads",
+               "seconds": round(wall, 2)}
 
     from public_b200 import cases
     from public_b200.cruna import Cruna, Settings
@@ -354,6 +374,19 @@ def traffic_from_profiles(kernel: str, n: int, precision: str):
     return None
 
 
+def relaunch(n: int) -> int:
+    """--gpus N without a launcher: start N ranks of this script through torch.distributed.run (one
+    process per GPU, rendezvous on 127.0.0.1) and return its status; rank 0 prints the JSON line."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), "--", *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -361,7 +394,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--ref-n", type=int, default=96)
+    ap.add_argument("--ref-n", type=int, default=0,
+                    help="grid of the CPU legs (default: --n, the benchmark's own configuration)")
+    ap.add_argument("--cpu-pairs", type=int, default=2, help="timed step pairs of the cpu_baseline leg")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--slabs", action="store_true",
@@ -369,6 +404,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the host-buffer run (grids whose staging would not fit beside the device working set)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch(args.gpus)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

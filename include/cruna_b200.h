@@ -4,7 +4,8 @@
  *
  * Every entry point replaces one Fortran module procedure of CRUNA (cruna-toolkit/public); the
  * procedure it stands in for is cited beside it as file:line.  A Fortran host binds these with
- * iso_c_binding (see the shim in INTEGRATION.md); Python binds them with ctypes.
+ * iso_c_binding (one interface block per entry point, arguments passed by value or as c_ptr);
+ * Python binds them with ctypes.
  *
  * Conventions
  *  - Arrays are Fortran-ordered (column-major) and contiguous: a field is f(n1,n2,n3), a state is
@@ -358,10 +359,14 @@ int64_t cruna_kernel_launches(const cruna_ctx *ctx);
    current device and the work is enqueued on `stream` (a cudaStream_t, NULL = default stream).
    Its intermediate (15 doubles per point) is a static device array of 131072 points (15.7 MB) that
    every GPU loading the library keeps until exit; larger grids are rejected with CRUNA_ERR_ARG.
-   The first call on a device resolves that array's address and sets kernel attributes: make it
-   before any stream capture.  All calls share the array, so calls that overlap on the GPU race;
-   serialise them (one stream, or events).  Each call overwrites every intermediate value it reads.
-   On failure a message is written to errbuf (errlen bytes, may be NULL). */
+   Every call resolves that array's address in the current context and sets the two kernels'
+   shared-memory limit (neither allocates).  The first call on a device also loads the library's
+   device code there; with lazy module loading that is when the array is mapped, so that call can fail
+   for lack of memory: make it at start-up, before any stream capture.  All calls share the array, so
+   calls that overlap on the GPU race; serialise them (one stream, or events).  Each call overwrites
+   every intermediate value it reads.  A CUDA error already pending on the calling thread is reported
+   (CRUNA_ERR_CUDA) and left pending, and nothing is launched.  On failure a message is written to
+   errbuf (errlen bytes, may be NULL). */
 int cruna_rhs_direct_noalloc(const cruna_config *cfg, const double *q, double *rhs, void *stream, char *errbuf,
                              int errlen);
 

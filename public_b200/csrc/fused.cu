@@ -419,15 +419,6 @@ size_t smem_d() {
   return sizeof(T) * (7 * (TX + 2 * R) * (TY + 2 * R) + ring_slots(R) * 4 * TX * TY);
 }
 
-int zchunk(const cruna_ctx *c, int bx, int by, int R, int &nz) {
-  const int n3 = c->g.n3;
-  nz = std::max(1, std::min(n3, (4 * 148 + bx * by - 1) / (bx * by)));
-  int kc = (n3 + nz - 1) / nz;
-  kc = std::max(kc, std::min(n3, 4 * R));
-  nz = (n3 + kc - 1) / kc;
-  return kc;
-}
-
 template <typename T, int R, bool PER>
 void launch_passes(cruna_ctx *c, FusedArgs &a) {
   static bool configured = false;
@@ -440,7 +431,7 @@ void launch_passes(cruna_ctx *c, FusedArgs &a) {
   }
   const int bx = (c->g.n1 + TX - 1) / TX, by = (c->g.n2 + TY - 1) / TY;
   int nz = 1;
-  a.kc = zchunk(c, bx, by, R, nz);
+  a.kc = z_chunk(c->g.n3, bx, by, R, nz);
   dim3 grid(bx, by, nz), block(TX, TY);
   {
     ProfScope ps(c, "pass_g");
@@ -583,9 +574,7 @@ namespace cruna {
 namespace {
 
 constexpr long long kNoAllocMaxPoints = 131072;          // e.g. 64 x 64 x 32 grid points
-constexpr int kNoAllocMaxDevices = 64;
 static __device__ __align__(256) double g_noalloc_scratch[NG * kNoAllocMaxPoints];
-double *g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};   // device address of the array, per device
 
 void noalloc_msg(char *buf, int len, const char *msg) {
   if (!buf || len <= 0) return;
@@ -594,19 +583,19 @@ void noalloc_msg(char *buf, int len, const char *msg) {
   buf[i] = 0;
 }
 
+// Sets the shared-memory limit of the two passes and launches them.  Called on every call: the
+// attribute belongs to the current context, which a host may have replaced since the last call.
 template <int R, bool PER>
-cudaError_t noalloc_attrs() {
+cudaError_t noalloc_launch(const FusedArgs &a, dim3 grid, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(k_pass_g<double, R, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem_g<double, R>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_pass_d<double, R, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_d<double, R>());
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_pass_d<double, R, PER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)smem_d<double, R>());
-}
-
-template <int R, bool PER>
-void noalloc_launch(const FusedArgs &a, dim3 grid, cudaStream_t s) {
   k_pass_g<double, R, PER><<<grid, dim3(TX, TY), smem_g<double, R>(), s>>>(a);
   k_pass_d<double, R, PER><<<grid, dim3(TX, TY), smem_d<double, R>(), s>>>(a);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -657,27 +646,23 @@ extern "C" int cruna_rhs_direct_noalloc(const cruna_config *cfg, const double *q
       return CRUNA_ERR_UNSUPPORTED;
     }
   }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
-    cudaGetLastError();
-    noalloc_msg(errbuf, errlen, "no usable current CUDA device");
-    return CRUNA_ERR_NODEVICE;
+  // an error left pending by the caller's earlier work would otherwise be read back (and cleared) as
+  // this call's failure: report it as such and launch nothing
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess) {
+    noalloc_msg(errbuf, errlen, "a CUDA error from earlier work is pending on this thread; nothing launched");
+    return CRUNA_ERR_CUDA;
   }
-  // first call on this device: resolve the array's device address and set the kernels' shared-memory
-  // limits (host code must not pass the array's name to a kernel: it is only a host-side stand-in)
-  if (!g_noalloc_ptr[dev]) {
-    void *ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (e == cudaSuccess) e = noalloc_attrs<2, false>();
-    if (e == cudaSuccess) e = noalloc_attrs<2, true>();
-    if (e == cudaSuccess) e = noalloc_attrs<4, false>();
-    if (e == cudaSuccess) e = noalloc_attrs<4, true>();
-    if (e != cudaSuccess || !ptr) {
-      cudaGetLastError();
-      noalloc_msg(errbuf, errlen, "cudaGetSymbolAddress / cudaFuncSetAttribute failed during set-up");
-      return CRUNA_ERR_CUDA;
-    }
-    g_noalloc_ptr[dev] = static_cast<double *>(ptr);
+  // the array's device address in the current context, resolved on every call (cheap, allocates
+  // nothing): host code must not pass the array's name to a kernel, it is only a host-side stand-in,
+  // and a cached address would go stale if the host switched contexts or reset the device
+  void *scratch = nullptr;
+  if (cudaGetSymbolAddress(&scratch, g_noalloc_scratch) != cudaSuccess || !scratch) {
+    const cudaError_t e = cudaGetLastError();
+    noalloc_msg(errbuf, errlen, e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver
+                                    ? "no usable current CUDA device"
+                                    : "cudaGetSymbolAddress of the static scratch array failed");
+    return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? CRUNA_ERR_NODEVICE : CRUNA_ERR_CUDA;
   }
   Grid g{cfg->n[0], cfg->n[1], cfg->n[2], npts};
   FusedArgs a;
@@ -695,7 +680,7 @@ extern "C" int cruna_rhs_direct_noalloc(const cruna_config *cfg, const double *q
   a.p_ref = 0.0;
   a.T_ref = 0.0;
   a.q = q;
-  a.gbuf = g_noalloc_ptr[dev];      // every value of the 15 fields is written by pass G before use
+  a.gbuf = scratch;                 // every value of the 15 fields is written by pass G before use
   a.rhs = rhs;
   a.force = nullptr;
   a.stage = 0;
@@ -709,20 +694,13 @@ extern "C" int cruna_rhs_direct_noalloc(const cruna_config *cfg, const double *q
   bool per = true;
   for (int d = 0; d < 3; ++d) per = per && ops[d].kind == OP_STENCIL && ops[d].periodic && ops[d].r == Rl;
   const int bx = (g.n1 + TX - 1) / TX, by = (g.n2 + TY - 1) / TY;
-  int nz = std::max(1, std::min(g.n3, (4 * 148 + bx * by - 1) / (bx * by)));
-  int kc = (g.n3 + nz - 1) / nz;
-  kc = std::max(kc, std::min(g.n3, 4 * Rl));
-  nz = (g.n3 + kc - 1) / kc;
-  a.kc = kc;
+  int nz = 1;
+  a.kc = z_chunk(g.n3, bx, by, Rl, nz);
+  const dim3 grid(bx, by, nz);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (Rl == 2) {
-    if (per) noalloc_launch<2, true>(a, dim3(bx, by, nz), s);
-    else noalloc_launch<2, false>(a, dim3(bx, by, nz), s);
-  } else {
-    if (per) noalloc_launch<4, true>(a, dim3(bx, by, nz), s);
-    else noalloc_launch<4, false>(a, dim3(bx, by, nz), s);
-  }
-  const cudaError_t e = cudaGetLastError();
+  cudaError_t e;
+  if (Rl == 2) e = per ? noalloc_launch<2, true>(a, grid, s) : noalloc_launch<2, false>(a, grid, s);
+  else e = per ? noalloc_launch<4, true>(a, grid, s) : noalloc_launch<4, false>(a, grid, s);
   if (e != cudaSuccess) {
     noalloc_msg(errbuf, errlen, cudaGetErrorString(e));
     return CRUNA_ERR_CUDA;

@@ -288,12 +288,8 @@ void launch_adj(cruna_ctx *c, AdjArgs &a) {
     configured = true;
   }
   const int bx = (c->g.n1 + TX - 1) / TX, by = (c->g.n2 + TY - 1) / TY;
-  const int n3 = c->g.n3;
-  int nz = std::max(1, std::min(n3, (4 * 148 + bx * by - 1) / (bx * by)));
-  int kc = (n3 + nz - 1) / nz;
-  kc = std::max(kc, std::min(n3, 4 * R));
-  nz = (n3 + kc - 1) / kc;
-  a.kc = kc;
+  int nz = 1;
+  a.kc = z_chunk(c->g.n3, bx, by, R, nz);
   ProfScope ps(c, "adj_pass");
   k_adj_pass<T, R, PER><<<dim3(bx, by, nz), dim3(TX, TY), smem_adj<T, R>(), c->stream>>>(a);
   CRUNA_LAUNCH_CHECK(c);

@@ -42,6 +42,20 @@ struct FusedArgs {
 
 __host__ __device__ constexpr int ring_slots(int R) { return 2 * R + 1; }
 
+// z-chunk length of one block of a z-marching kernel on a (bx, by) grid of plane tiles: enough chunks
+// that the grid covers at least 4 blocks per SM of the 148, each chunk at least 4R planes long (the
+// ring start-up reads 2R planes).  nz receives the number of chunks.
+inline int z_chunk(int n3, int bx, int by, int R, int &nz) {
+  nz = n3 < 1 ? 1 : (4 * 148 + bx * by - 1) / (bx * by);
+  if (nz > n3) nz = n3;
+  if (nz < 1) nz = 1;
+  int kc = (n3 + nz - 1) / nz;
+  const int kmin = n3 < 4 * R ? n3 : 4 * R;
+  if (kc < kmin) kc = kmin;
+  nz = (n3 + kc - 1) / kc;
+  return kc;
+}
+
 template <typename T, int R>
 __device__ __forceinline__ T dsm(const DirOpF &op, const T *p, int s, int i) {
   // derivative (unscaled) at line position i; p points at the point, neighbours at p[m*s]

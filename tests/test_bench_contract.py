@@ -31,3 +31,18 @@ def test_reference_arm_other_ranks_are_silent():
     lines = run_bench({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"},
                       "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--ref-n", "24")
     assert lines == []
+
+
+def test_gpus_flag_launches_the_ranks_itself():
+    """`bench.py --gpus 2` without a launcher starts two ranks through torch.distributed.run; the
+    reference arm's rank 0 alone prints, so the run yields exactly one JSON line with n_gpus 2."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "0", "--n", "16"], cwd=ROOT, env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1, lines
+    out = json.loads(lines[0])
+    assert out["impl"] == "reference" and out["n_gpus"] == 2 and out["config"]["same_config"] is True
+    assert abs(out["ms_per_step"] / 1e3 - 16 ** 3 / out["value"]) < 1e-9 * out["ms_per_step"]

@@ -75,3 +75,36 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     err = C.create_string_buffer(256)
     rc = lib.cruna_rhs_direct_noalloc(C.byref(cfg), C.c_void_p(16), C.c_void_p(16), None, err, 256)
     assert rc == -1 and b"131072" in err.value
+
+
+def test_noalloc_orders_its_work_on_the_callers_stream():
+    """The work is enqueued on the stream the caller passes: q is written on a side stream just before
+    the call, only that stream is synchronised, and the result still matches the context RHS."""
+    import torch
+
+    s, q = cases.taylor_green(n=16, seed=6)
+    s["mu0"] = 0.01
+    st = Settings.from_dict(s)
+    dev = torch.device("cuda", 0)
+    q_host = torch.from_numpy(np.ascontiguousarray(q.ravel(order="F"))).pin_memory()
+    qd = torch.from_numpy(np.ascontiguousarray(q.ravel(order="F"))).to(dev)
+    r_ref = torch.empty_like(qd)
+    with Cruna(st) as c:
+        c.rhs_direct_dev(qd.data_ptr(), r_ref.data_ptr())
+        c.sync()
+        lib = c.lib
+        cfg = st.to_struct(lib)
+    side = torch.cuda.Stream(device=dev)
+    q_side = torch.zeros_like(qd)
+    r_new = torch.full_like(qd, float("nan"))
+    torch.cuda.synchronize()
+    err = C.create_string_buffer(256)
+    with torch.cuda.stream(side):
+        q_side.copy_(q_host, non_blocking=True)       # q arrives on the side stream only
+        rc = lib.cruna_rhs_direct_noalloc(C.byref(cfg), C.c_void_p(q_side.data_ptr()),
+                                          C.c_void_p(r_new.data_ptr()), C.c_void_p(side.cuda_stream), err, 256)
+    assert rc == 0, err.value.decode()
+    side.synchronize()
+    a = r_new.cpu().numpy().reshape(st.n + (5,), order="F")
+    b = r_ref.cpu().numpy().reshape(st.n + (5,), order="F")
+    _check(a, b)
