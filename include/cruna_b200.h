@@ -39,6 +39,8 @@ extern "C" {
 #define CRUNA_ERR_STATE (-4)     /* non-finite or non-physical state detected (rho <= 0, p <= 0, NaN) */
 #define CRUNA_ERR_UNSUPPORTED (-5) /* boundary type / scheme / path not available */
 #define CRUNA_ERR_NODEVICE (-6)  /* no CUDA device */
+#define CRUNA_STOPPED 1          /* cruna_run_hpc: stopped by its wall-time or step budget after storing
+                                    a snapshot and the restart file (not an error) */
 
 /* derivative cores (selected at compile time in CRUNA by discretisation_x_core.f90) */
 enum cruna_diff_scheme {
@@ -369,6 +371,58 @@ int64_t cruna_kernel_launches(const cruna_ctx *ctx);
    errbuf (errlen bytes, may be NULL). */
 int cruna_rhs_direct_noalloc(const cruna_config *cfg, const double *q, double *rhs, void *stream, char *errbuf,
                              int errlen);
+
+/*
+ * Snapshot / restart files and the direct main loop with restart (src/main/cruna_hpc.f90:99-299).
+ * The reference writes HDF5 (src/io/hdf5_single.f90:659-774: dataset "data" (n1,n2,n3,5) FP64 plus
+ * "params"); this library writes the same content in a flat binary container under the reference's
+ * file names (src/helper/io_helper.f90:11-15, 426-432) with ".bin" in place of ".h5":
+ *   data_direct_snapshot__BB_IIIII_SS_TTTTTTT.bin   (world block, block image, subset, time step)
+ *   restartfile.bin                                 (the int32 pair (ns, nt) of the last restart point)
+ * Layout: 64-byte header (magic "CRUNAB2D", int32 version 1, int32 element size 8 or 4, int64 dims[4],
+ * int64 params length, int64 0), the params text ("key = value" lines), the data in Fortran order.
+ * Files are written to "<name>.tmp" and renamed.  Context-free functions report errors through
+ * cruna_last_error(NULL).
+ */
+/* Writes the file name of `type` ("data_direct_snapshot", "data_adjoint_snapshot", "data_direct",
+   "data_adjoint", "restartfile") into buf; returns its length (or a negative error). */
+int cruna_io_fname(char *buf, int buflen, const char *workdir, const char *type, int world_block, int block_image,
+                   int ns, int nt);
+/* store_4d_rk (hdf5_single.f90:659-774) / its load: dims = Fortran shape; on read, dims is checked against
+   the file when data is non-NULL, else filled from it (params, if given, receives the params text). */
+int cruna_write_snapshot(const char *path, const int64_t dims[4], const double *data, const char *params);
+int cruna_read_snapshot(const char *path, int64_t dims[4], double *data, char *params, int params_len);
+/* restartfile with (ns, nt) (cruna_hpc.f90:196-199); read returns 1 when found, 0 when the file does not
+   exist (the reference then starts from 0, :127-131), negative on error */
+int cruna_write_restart(const char *workdir, int ns, int nt);
+int cruna_read_restart(const char *workdir, int *ns, int *nt);
+/* First subset and step after a restart point (cruna_hpc.f90:143-145):
+   nt_total = (ns-1)*steps + nt + 1, s0 = nt_total/steps + 1, nt0 = nt_total - (s0-1)*steps. */
+int cruna_restart_start(int ns, int nt, int steps, int *s0, int *nt0);
+/* data_direct_snapshot of the context's grid at (ns, nt) from / to a HOST state (n1*n2*n3*5 doubles). */
+int cruna_store_snapshot(cruna_ctx *ctx, const char *workdir, const char *type, const double *q, int ns, int nt);
+int cruna_load_snapshot(cruna_ctx *ctx, const char *workdir, const char *type, double *q, int ns, int nt);
+
+typedef struct cruna_hpc_opts {
+  const char *workdir;   /* io.workdirectory (NULL or "" = ".") */
+  int32_t steps;         /* time.steps: steps per subset */
+  int32_t subsets;       /* time.subsets */
+  int32_t dsfreq;        /* io.dsfreq: snapshot + restart file every dsfreq steps, and the initial and
+                            final snapshots; <= 0: no files except at a budget stop */
+  int32_t restart;       /* init.restart: continue from restartfile.bin when it exists */
+  double walltime;       /* run.walltime in seconds of elapsed time (the reference: hours of CPU time);
+                            <= 0: none */
+  int32_t max_steps;     /* steps this call may take (<= 0: unlimited); reaching it acts like the wall time */
+  int32_t reserved;
+} cruna_hpc_opts;
+/* The direct main loop of cruna_hpc (cruna_hpc.f90:99-299): store the initial condition as snapshot
+   (1, 0), on restart load (ns, nt) from restartfile.bin and the matching snapshot, then run the subset
+   and step loops from cruna_restart_start (time_stepper_direct, BC q outside, filters on the step index
+   within the subset), storing a snapshot and the restart file every dsfreq steps; when the wall-time or
+   step budget runs out before the end, store both at the current step and return CRUNA_STOPPED.  As in
+   the reference, nt0 applies to every subset after a restart.  q_io (HOST) holds the initial condition
+   on entry and the last state on return; *ns_out / *nt_out receive the last (subset, step) done. */
+int cruna_run_hpc(cruna_ctx *ctx, double *q_io, const cruna_hpc_opts *opts, int *ns_out, int *nt_out);
 
 /* Kernel timing: while enabled, each kernel family (fused passes, filters, stage updates, generic
    line operators) is bracketed by CUDA events on the context's stream.  cruna_profile_report drains

@@ -40,6 +40,7 @@ FILTER = {"empty": 0, "o2_i_c_p": 1, "o6_i_c_p": 2, "o2_i_c_o": 3, "o4_i_c_o": 4
 PRECISION = {"fp64": 0, "fp32": 1}
 ABI_VERSION = 2
 
+CRUNA_STOPPED = 1
 ERRORS = {-1: "CRUNA_ERR_ARG", -2: "CRUNA_ERR_CUDA", -3: "CRUNA_ERR_NOMEM", -4: "CRUNA_ERR_STATE",
           -5: "CRUNA_ERR_UNSUPPORTED", -6: "CRUNA_ERR_NODEVICE"}
 
@@ -71,6 +72,13 @@ class Objective(C.Structure):
 _P = C.c_void_p
 _D = C.c_double
 _I = C.c_int
+
+class HpcOpts(C.Structure):
+    """cruna_hpc_opts: the keys of cruna_hpc's main loop (src/main/cruna_hpc.f90:99-299)."""
+    _fields_ = [("workdir", C.c_char_p), ("steps", C.c_int32), ("subsets", C.c_int32), ("dsfreq", C.c_int32),
+                ("restart", C.c_int32), ("walltime", C.c_double), ("max_steps", C.c_int32),
+                ("reserved", C.c_int32)]
+
 
 _SIGNATURES = {
     "cruna_config_defaults": (None, [C.POINTER(_Config)]),
@@ -149,6 +157,15 @@ _SIGNATURES = {
                                 C.POINTER(C.c_int64)]),
     "cruna_lapack_dgttrf": (_I, [_I, _P, _P, _P, _P, _P]),
     "cruna_lapack_dgttrs": (None, [_I, _P, _P, _P, _P, _P, _P]),
+    "cruna_io_fname": (_I, [C.c_char_p, _I, C.c_char_p, C.c_char_p, _I, _I, _I, _I]),
+    "cruna_write_snapshot": (_I, [C.c_char_p, C.POINTER(C.c_int64), _P, C.c_char_p]),
+    "cruna_read_snapshot": (_I, [C.c_char_p, C.POINTER(C.c_int64), _P, C.c_char_p, _I]),
+    "cruna_write_restart": (_I, [C.c_char_p, _I, _I]),
+    "cruna_read_restart": (_I, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "cruna_restart_start": (_I, [_I, _I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "cruna_store_snapshot": (_I, [_P, C.c_char_p, C.c_char_p, _P, _I, _I]),
+    "cruna_load_snapshot": (_I, [_P, C.c_char_p, C.c_char_p, _P, _I, _I]),
+    "cruna_run_hpc": (_I, [_P, _P, C.POINTER(HpcOpts), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
 }
 
 _lib = None
@@ -602,3 +619,83 @@ class Cruna:
 
     def stream_handle(self) -> int:
         return int(self.lib.cruna_stream(self.h) or 0)
+
+    # ---- snapshots and restart (src/main/cruna_hpc.f90:99-299, src/helper/io_helper.f90) -------
+    def store_snapshot(self, q, workdir: str, ns: int, nt: int, kind: str = "data_direct_snapshot"):
+        a = self._state(q)
+        self._check(self.lib.cruna_store_snapshot(self.h, workdir.encode(), kind.encode(), _ptr(a), ns, nt))
+
+    def load_snapshot(self, workdir: str, ns: int, nt: int, kind: str = "data_direct_snapshot") -> np.ndarray:
+        a = np.zeros(self.n + (5,), order="F")
+        self._check(self.lib.cruna_load_snapshot(self.h, workdir.encode(), kind.encode(), _ptr(a), ns, nt))
+        return a
+
+    def run_hpc(self, q0, workdir: str, steps: int, subsets: int = 1, dsfreq: int = 0, restart: bool = False,
+                walltime: float = 0.0, max_steps: int = 0):
+        """cruna_hpc's direct main loop with snapshots and restart; returns (q, stopped, (ns, nt)):
+        stopped is True when the wall-time or step budget ended the call after storing a restart point."""
+        a = np.array(self._state(q0), order="F", copy=True)
+        o = HpcOpts(workdir.encode(), int(steps), int(subsets), int(dsfreq), 1 if restart else 0, float(walltime),
+                    int(max_steps), 0)
+        ns, nt = C.c_int(), C.c_int()
+        rc = self.lib.cruna_run_hpc(self.h, _ptr(a), C.byref(o), C.byref(ns), C.byref(nt))
+        if rc not in (0, CRUNA_STOPPED):
+            self._check(rc)
+        return a, rc == CRUNA_STOPPED, (ns.value, nt.value)
+
+
+def _io_check(lib, rc: int) -> int:
+    if rc < 0:
+        raise CrunaError(rc, lib.cruna_last_error(None).decode())
+    return rc
+
+
+def io_fname(workdir: str, kind: str, ns: int = 1, nt: int = 0, world_block: int = 1, block_image: int = 1) -> str:
+    """The reference's file name of a snapshot / restart file (src/helper/io_helper.f90:11-432), '.bin'."""
+    lib = load_library()
+    n = _io_check(lib, lib.cruna_io_fname(None, 0, workdir.encode(), kind.encode(), world_block, block_image, ns,
+                                          nt))
+    buf = C.create_string_buffer(n + 1)
+    lib.cruna_io_fname(buf, n + 1, workdir.encode(), kind.encode(), world_block, block_image, ns, nt)
+    return buf.value.decode()
+
+
+def write_snapshot(path: str, data: np.ndarray, params: str = ""):
+    """store_4d_rk (src/io/hdf5_single.f90:659-774) in the library's binary container."""
+    lib = load_library()
+    a = np.asfortranarray(np.asarray(data, dtype=np.float64))
+    shape = tuple(a.shape) + (1,) * (4 - a.ndim)
+    dims = (C.c_int64 * 4)(*shape)
+    _io_check(lib, lib.cruna_write_snapshot(path.encode(), dims, _ptr(a), params.encode()))
+
+
+def read_snapshot(path: str) -> Tuple[np.ndarray, str]:
+    """The data (Fortran order, 4-D) and the params text of a snapshot file."""
+    lib = load_library()
+    dims = (C.c_int64 * 4)(0, 0, 0, 0)
+    _io_check(lib, lib.cruna_read_snapshot(path.encode(), dims, None, None, 0))
+    a = np.zeros(tuple(dims), order="F")
+    txt = C.create_string_buffer(1 << 16)
+    _io_check(lib, lib.cruna_read_snapshot(path.encode(), dims, _ptr(a), txt, 1 << 16))
+    return a, txt.value.decode()
+
+
+def write_restart(workdir: str, ns: int, nt: int):
+    lib = load_library()
+    _io_check(lib, lib.cruna_write_restart(workdir.encode(), int(ns), int(nt)))
+
+
+def read_restart(workdir: str) -> Optional[Tuple[int, int]]:
+    """(ns, nt) of restartfile.bin, or None when there is none (the reference then starts from 0)."""
+    lib = load_library()
+    ns, nt = C.c_int(), C.c_int()
+    found = _io_check(lib, lib.cruna_read_restart(workdir.encode(), C.byref(ns), C.byref(nt)))
+    return (ns.value, nt.value) if found == 1 else None
+
+
+def restart_start(ns: int, nt: int, steps: int) -> Tuple[int, int]:
+    """(s0, nt0) after restart point (ns, nt): src/main/cruna_hpc.f90:143-145."""
+    lib = load_library()
+    s0, nt0 = C.c_int(), C.c_int()
+    _io_check(lib, lib.cruna_restart_start(int(ns), int(nt), int(steps), C.byref(s0), C.byref(nt0)))
+    return s0.value, nt0.value

@@ -305,6 +305,14 @@ void cruna_config_defaults(cruna_config *cfg) {
   cfg->check_every = 0;
 }
 
+}  // extern "C"
+
+namespace cruna {
+void set_global_error(const std::string &msg) { g_init_error = msg; }
+}  // namespace cruna
+
+extern "C" {
+
 const char *cruna_last_error(const cruna_ctx *ctx) {
   return ctx ? ctx->err.c_str() : g_init_error.c_str();
 }
