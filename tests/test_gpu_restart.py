@@ -51,6 +51,7 @@ def settings():
 @pytest.mark.parametrize("subsets,steps,stop", [(1, 12, 5), (2, 6, 6), (2, 6, 9)])
 def test_run_split_across_two_processes_is_bit_identical(tmp_path, subsets, steps, stop):
     s, q0 = settings()
+    (tmp_path / "one").mkdir()
     with Cruna(Settings.from_dict(s)) as c:
         full, stopped, pos = c.run_hpc(q0, str(tmp_path / "one"), steps=steps, subsets=subsets, dsfreq=4)
         assert not stopped and pos == (subsets, steps)
