@@ -226,6 +226,8 @@ def run_ours(args):
     st.device = local
     st.precision = args.precision
     ctx = Cruna(st)
+    if args.tma:
+        ctx.tma_passes(True)
     if slabs is not None:
         slabs.attach(ctx)
     N = args.n ** 3                                   # interior points of this rank
@@ -401,6 +403,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--slabs", action="store_true",
                     help="z-slab decomposition with halo exchange also on one GPU (the path --gpus N runs)")
+    ap.add_argument("--tma", action="store_true",
+                    help="FP64 adjoint pass fed by TMA instead of the per-thread-load kernel (the default)")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the host-buffer run (grids whose staging would not fit beside the device working set)")
     args = ap.parse_args()

@@ -348,6 +348,11 @@ int cruna_check_state_dev(cruna_ctx *ctx, const double *q);
    sequence (compact schemes, 204/200 boundary types).  force_generic=1 selects the generic one. */
 int cruna_rhs_path(const cruna_ctx *ctx);
 int cruna_set_force_generic(cruna_ctx *ctx, int force_generic);
+/* FP64 fused adjoint pass: on = 1 feeds it by TMA (cp.async.bulk.tensor tiles, column boxes and RK
+   inputs into shared memory, z columns in registers) where the layout allows it (n1 even, 16-byte
+   aligned states); on = 0 (default) keeps the per-thread-load kernel, which measures faster on B200
+   (1.35 against 1.40 ms per launch at 256^3).  Both give the same results to rounding. */
+int cruna_set_tma_passes(cruna_ctx *ctx, int on);
 
 /* Number of kernels this library enqueued since the context was created (for launch accounting). */
 int64_t cruna_kernel_launches(const cruna_ctx *ctx);

@@ -119,6 +119,7 @@ _SIGNATURES = {
     "cruna_check_state_dev": (_I, [_P, _P]),
     "cruna_rhs_path": (_I, [_P]),
     "cruna_set_force_generic": (_I, [_P, _I]),
+    "cruna_set_tma_passes": (_I, [_P, _I]),
     "cruna_kernel_launches": (C.c_int64, [_P]),
     "cruna_profile_enable": (_I, [_P, _I]),
     "cruna_profile_report": (_I, [_P, C.c_char_p, _I]),
@@ -324,6 +325,10 @@ class Cruna:
 
     def force_generic(self, on: bool = True):
         self._check(self.lib.cruna_set_force_generic(self.h, 1 if on else 0))
+
+    def tma_passes(self, on: bool = True):
+        """FP64 fused adjoint pass fed by TMA, or by per-thread loads (the default, faster on B200)."""
+        self._check(self.lib.cruna_set_tma_passes(self.h, 1 if on else 0))
 
     @property
     def launches(self) -> int:
@@ -561,6 +566,11 @@ class Cruna:
 
     def step_direct_dev(self, q0_ptr: int, q1_ptr: int, t: float = 0.0):
         self._check(self.lib.cruna_step_direct_dev(self.h, C.c_void_p(q0_ptr), C.c_void_p(q1_ptr), float(t)))
+
+    def step_adjoint_dev(self, qs0_ptr: int, q0_ptr: int, g_ptr: Optional[int], qs1_ptr: int, t: float = 0.0):
+        self._check(self.lib.cruna_step_adjoint_dev(self.h, C.c_void_p(qs0_ptr), C.c_void_p(q0_ptr),
+                                                    None if g_ptr is None else C.c_void_p(g_ptr),
+                                                    C.c_void_p(qs1_ptr), float(t)))
 
     def run_direct_dev(self, q_ptr: int, nt0: int, nsteps: int, traj_ptr: Optional[int] = None):
         self._check(self.lib.cruna_run_direct_dev(self.h, C.c_void_p(q_ptr), int(nt0), int(nsteps),

@@ -572,6 +572,12 @@ int cruna_set_force_generic(cruna_ctx *c, int v) {
   return CRUNA_OK;
 }
 
+int cruna_set_tma_passes(cruna_ctx *c, int on) {
+  if (!c) return CRUNA_ERR_ARG;
+  c->tma_fused = on != 0;
+  return CRUNA_OK;
+}
+
 int64_t cruna_kernel_launches(const cruna_ctx *c) { return c ? c->launches : -1; }
 
 int cruna_set_reference_dev(cruna_ctx *c, const double *qref) {

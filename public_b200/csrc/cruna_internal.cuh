@@ -126,6 +126,7 @@ struct cruna_ctx {
   std::string err;
   bool force_generic = false;
   bool fused_ok = false;
+  bool tma_fused = false;       // FP64 adjoint pass fed by TMA where the layout allows (cruna_set_tma_passes)
   bool filter_fused_ok = false;
   // FP32-stencil path: pressure / temperature offsets differenced in FP32 (set once per context)
   bool refs_set = false;

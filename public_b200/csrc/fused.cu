@@ -430,17 +430,20 @@ void launch_passes(cruna_ctx *c, FusedArgs &a) {
     configured = true;
   }
   const int bx = (c->g.n1 + TX - 1) / TX, by = (c->g.n2 + TY - 1) / TY;
+  static const int res_g = resident_blocks(k_pass_g<T, R, PER>, TX * TY, smem_g<T, R>());
+  static const int res_d = resident_blocks(k_pass_d<T, R, PER>, TX * TY, smem_d<T, R>());
+  const int sms = device_sms();
   int nz = 1;
-  a.kc = z_chunk(c->g.n3, bx, by, R, nz);
-  dim3 grid(bx, by, nz), block(TX, TY);
   {
+    a.kc = z_chunk_balanced(c->g.n3, bx * by, res_g, sms, R, nz);
     ProfScope ps(c, "pass_g");
-    k_pass_g<T, R, PER><<<grid, block, smem_g<T, R>(), c->stream>>>(a);
+    k_pass_g<T, R, PER><<<dim3(bx, by, nz), dim3(TX, TY), smem_g<T, R>(), c->stream>>>(a);
     CRUNA_LAUNCH_CHECK(c);
   }
   {
+    a.kc = z_chunk_balanced(c->g.n3, bx * by, res_d, sms, R, nz);
     ProfScope ps(c, "pass_d");
-    k_pass_d<T, R, PER><<<grid, block, smem_d<T, R>(), c->stream>>>(a);
+    k_pass_d<T, R, PER><<<dim3(bx, by, nz), dim3(TX, TY), smem_d<T, R>(), c->stream>>>(a);
     CRUNA_LAUNCH_CHECK(c);
   }
 }

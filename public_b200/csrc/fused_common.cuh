@@ -2,7 +2,12 @@
 // the derivative evaluators on shared-memory rows (x, y) and register columns (z).
 #pragma once
 
+#include <cuda.h>
+
+#include <cmath>
+
 #include "cruna_internal.cuh"
+#include "tcgen05.cuh"
 
 namespace cruna {
 namespace fz {
@@ -54,6 +59,61 @@ inline int z_chunk(int n3, int bx, int by, int R, int &nz) {
   if (kc < kmin) kc = kmin;
   nz = (n3 + kc - 1) / kc;
   return kc;
+}
+
+// z-chunking balanced against the launch waves: `tiles` plane tiles, `resident` blocks of the kernel per
+// SM and `sms` SMs.  Among the chunk counts whose chunks stay at least 4R planes long it picks the one
+// that maximises the filled fraction of the last wave times kc / (kc + R/2) (each chunk first reads 2R
+// planes, about a quarter of a marching step each).  Returns kc; nz receives the number of chunks.
+inline int z_chunk_balanced(int n3, int tiles, int resident, int sms, int R, int &nz) {
+  if (resident < 1 || sms < 1 || tiles < 1) return z_chunk(n3, 1, tiles, R, nz);
+  const int kmin = n3 < 4 * R ? n3 : 4 * R;
+  double best = -1.0;
+  int best_kc = n3;
+  nz = 1;
+  for (int z = 1; z <= n3 && z <= 256; ++z) {
+    const int kc = (n3 + z - 1) / z;
+    if (kc < kmin) break;
+    const int nzr = (n3 + kc - 1) / kc;
+    const double waves = (double)tiles * nzr / ((double)resident * sms);
+    const double eff = waves / std::ceil(waves) * (double)kc / (kc + 0.5 * R);
+    if (eff > best + 1e-9) {
+      best = eff;
+      best_kc = kc;
+      nz = nzr;
+    }
+  }
+  return best_kc;
+}
+
+// SM count of the current device (cached per device ordinal)
+inline int device_sms() {
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return 148;
+  }
+  if (!cache[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v < 1) {
+      cudaGetLastError();
+      v = 148;
+    }
+    cache[dev] = v;
+  }
+  return cache[dev];
+}
+
+// resident blocks per SM of a kernel at a launch shape (0 when the query fails)
+template <typename K>
+int resident_blocks(K kernel, int threads, size_t smem) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nb;
 }
 
 template <typename T, int R>
@@ -271,6 +331,36 @@ struct HaloSet {
 
 DirOpF to_dir(const LineOp &op, double dx, bool heat_dx);
 int halo_of(const LineOp &op);
+
+// ---- TMA plumbing of the fused passes ------------------------------------------------------------
+// Bounded spin of an mbarrier wait (iterations of try_wait); a block whose wait runs out records it in
+// the context's error flag, waits (again bounded) for its copies in flight and returns.
+constexpr long long kTmaSpinLimit = 1LL << 22;
+
+// 4-D tensor map (x, y, z, field) over nf Fortran-ordered fields of n1 x n2 x n3 doubles, fields
+// fstride elements apart, with a (bx, by, 1, bf) box; false when the layout does not meet TMA's rules
+// (16-byte aligned base, row / plane / field strides multiples of 16 bytes, i.e. n1 even).
+bool tma_field_map(const double *base, int n1, int n2, int n3, int nf, long long fstride, int bx, int by, int bf,
+                   CUtensorMap *tm);
+
+// this thread's arrival on `bar` announcing `bytes` of TMA writes
+__device__ __forceinline__ void tma_expect(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// plain arrival (a phase without copies)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_addr(bar)) : "memory");
+}
+// box at (x, y, z, f) of the map into dst (this CTA's shared memory), completion counted on bar
+__device__ __forceinline__ void tma_load4(const CUtensorMap *tm, void *dst, uint64_t *bar, int x, int y, int z,
+                                          int f) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(tc::smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(f), "r"(tc::smem_addr(bar))
+      : "memory");
+}
 
 }  // namespace fz
 }  // namespace cruna

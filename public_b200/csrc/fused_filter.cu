@@ -226,6 +226,31 @@ bool state_tensor_map(const cruna_ctx *c, const double *state, CUtensorMap *tm) 
 
 }  // namespace
 
+namespace fz {
+bool tma_field_map(const double *base, int n1, int n2, int n3, int nf, long long fstride, int bx, int by, int bf,
+                   CUtensorMap *tm) {
+  if (n1 % 2 != 0 || fstride % 2 != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+  if (bx < 1 || bx > 256 || by < 1 || by > 256 || bf < 1 || bf > 256 || (bx * 8) % 16 != 0) return false;
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      cudaGetLastError();
+      return false;
+    }
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[4] = {(cuuint64_t)n1, (cuuint64_t)n2, (cuuint64_t)n3, (cuuint64_t)nf};
+  const cuuint64_t strides[3] = {(cuuint64_t)n1 * 8, (cuuint64_t)n1 * n2 * 8, (cuuint64_t)fstride * 8};
+  const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)bf}, elem[4] = {1, 1, 1, 1};
+  return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double *>(base), dims, strides, box, elem,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+}  // namespace fz
+
 // filters usable by the fused passes: the explicit periodic o10 filter or none, in every direction
 bool filter_fused_supported(const cruna_ctx *c) {
   double ref[FR + 1] = {0};
