@@ -320,6 +320,14 @@ int cruna_set_closure_normalisation(cruna_ctx *ctx, int on);
    -d_j tau_ij(model) to the momentum equations, on top of the forcing set with cruna_set_forcing.  The
    MLP must outlive the attachment; the discrete adjoint (mode 1) is unavailable while attached. */
 int cruna_set_closure(cruna_ctx *ctx, cruna_mlp *mlp, double delta);
+/* Where the attached closure runs on the fused (explicit-scheme) RHS path: on = 1 (default) inside the
+   flux pass -- the pass that forms the viscous stresses evaluates the network on the tensor cores for
+   each plane tile of 128 points (features from its own velocity gradients, BF16 operands, FP32
+   accumulators in TMEM) and subtracts the model stresses from the stresses it writes, so the
+   divergence pass differentiates both at once; on = 0 as separate launches (features, network, stress
+   divergence) through the forcing hook.  The generic path always uses the separate launches.  Both
+   agree up to the BF16 rounding of the network's inputs. */
+int cruna_set_closure_fused(cruna_ctx *ctx, int on);
 
 /* J of the objective after nsteps direct loop steps from q0 (calc_direct + calc_objective,
    cruna.f90:90-117), without the adjoint: what finite-difference checks and line searches evaluate. */

@@ -142,6 +142,7 @@ _SIGNATURES = {
     "cruna_box_filter_dev": (_I, [_P, _I, _P, _P, _P]),
     "cruna_closure_features_dev": (_I, [_P, _P, C.c_double, _P]),
     "cruna_set_closure": (_I, [_P, _P, C.c_double]),
+    "cruna_set_closure_fused": (_I, [_P, _I]),
     "cruna_set_halo_exchange": (_I, [_P, _P, _P]),
     "cruna_objective_value": (_I, [_P, _P, _I, C.POINTER(Objective), C.POINTER(C.c_double)]),
     "cruna_objective_value_dev": (_I, [_P, _P, _I, C.POINTER(Objective), C.POINTER(C.c_double)]),
@@ -476,6 +477,10 @@ class Cruna:
     def set_closure_normalisation(self, on: bool = True):
         """Scale-free closure features and outputs (grad u / |grad u|, |grad u| delta; tau / (rho (|grad u| delta)^2))."""
         self._check(self.lib.cruna_set_closure_normalisation(self.h, 1 if on else 0))
+
+    def set_closure_fused(self, on: bool = True):
+        """Closure evaluated inside the flux pass (default) or by separate launches."""
+        self._check(self.lib.cruna_set_closure_fused(self.h, 1 if on else 0))
 
     def set_closure(self, mlp, delta: float = 0.0):
         """Attach a public_b200.closure.ClosureMLP (None detaches)."""

@@ -127,6 +127,10 @@ void ensure_closure_buffers(cruna_ctx *c) {
 
 void closure_stage(cruna_ctx *c, const double *q) {
   if (!c->closure_mlp) return;
+  if (closure_in_pass(c)) {                        // pass G adds the model stresses itself
+    c->force = c->user_force;
+    return;
+  }
   const long long N = c->g.N;
   features(c, q, c->closure_delta, c->cl_x);
   mlp_forward_stream(c->closure_mlp, c->cl_x, c->cl_y, N, c->stream);
@@ -193,6 +197,13 @@ int cruna_closure_features_dev(cruna_ctx *c, const double *q, double delta, floa
   return closure_guard(c, [&]() -> int {
     if (!q || !X) throw ApiError{CRUNA_ERR_ARG, "null pointer"};
     features(c, q, delta, X);
+    return CRUNA_OK;
+  });
+}
+
+int cruna_set_closure_fused(cruna_ctx *c, int on) {
+  return closure_guard(c, [&]() -> int {
+    c->closure_fused = on != 0;                    // closure_stage picks the forcing before each RHS
     return CRUNA_OK;
   });
 }

@@ -169,6 +169,7 @@ struct cruna_ctx {
   struct cruna_mlp *closure_mlp = nullptr;
   double closure_delta = 0.0;
   bool closure_norm = false;       // scale-free features / outputs (cruna_set_closure_normalisation)
+  bool closure_fused = true;       // network evaluated inside the fused pass G (cruna_set_closure_fused)
   double *user_force = nullptr;    // the caller's forcing (cruna_set_forcing) while a closure is set
   double *cl_force = nullptr;      // forcing + closure stress divergence (5N)
   double *cl_tau = nullptr;        // model stresses (6N) and their derivatives (9N)
@@ -242,6 +243,7 @@ bool use_fused(const cruna_ctx *c);
 // learned closure (closure_mlp.cu, closure_ops.cu)
 void mlp_forward_stream(struct cruna_mlp *h, const float *X, float *Y, long long n, cudaStream_t stream);
 void closure_stage(cruna_ctx *c, const double *q);  // sets c->force for the next direct RHS evaluation
+bool closure_in_pass(const cruna_ctx *c);           // the fused pass G evaluates the closure itself
 // discrete adjoint (discrete_adjoint.cu)
 void rhs_direct_vjp(cruna_ctx *c, const double *q, const double *lam, double *mu, double *gf_acc);
 void step_direct_vjp(cruna_ctx *c, const double *q0, const double *lam1, double *lam0, double *gf_acc,

@@ -34,12 +34,34 @@ namespace {
 // pass G
 // plane fields: 0 u, 1 v, 2 w, 3 T', 4 p', 5 rho*u, 6 rho*v ; ring fields: 0 u, 1 v, 2 w, 3 T', 4 p', 5 rho*w
 // ------------------------------------------------------------------------------------------------
-template <typename T, int R, bool PER>
+// Shared memory of the closure part of pass G: BF16 weights in the tcgen05 K-major layout, biases,
+// the MMA mbarrier and the TMEM address; the activation tiles X [128][16] and H [128][64] reuse the
+// plane when it is large enough (FP64), else follow this block.
+struct ClSmem {
+  __nv_bfloat16 W1[mlp::HID * 16];
+  __nv_bfloat16 W2[mlp::HID * mlp::HID];
+  __nv_bfloat16 W3[16 * mlp::HID];
+  float b1[mlp::HID], b2[mlp::HID], b3[16];
+  uint64_t mbar;
+  uint32_t tmem;
+};
+constexpr size_t kClActBytes = (128 * 16 + 128 * mlp::HID) * sizeof(__nv_bfloat16);
+
+template <typename T, int R>
+constexpr size_t plane_bytes_g() { return sizeof(T) * 7 * (TX + 2 * R) * (TY + 2 * R); }
+template <typename T, int R>
+constexpr size_t ring_bytes_g() { return sizeof(T) * ring_slots(R) * 6 * TX * TY; }
+template <typename T, int R>
+constexpr size_t cl_offset_g() { return ((plane_bytes_g<T, R>() + ring_bytes_g<T, R>() + 1023) / 1024) * 1024; }
+template <typename T, int R>
+constexpr bool cl_alias_plane() { return plane_bytes_g<T, R>() >= kClActBytes; }
+
+template <typename T, int R, bool PER, bool CL = false>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_pass_g(const __grid_constant__ FusedArgs a) {
   constexpr int PW = TX + 2 * R, PH = TY + 2 * R, PS = PW * PH;
   constexpr int NS = ring_slots(R);
   constexpr int NRF = 6, RS = TX * TY;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   T *plane = reinterpret_cast<T *>(smem_raw);          // [7][PH][PW]
   T *ring = plane + 7 * PS;                            // [NS][NRF][TY*TX]
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -56,6 +78,29 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_pass_g(const
   const double *Q0 = a.q, *Q1 = a.q + N, *Q2 = a.q + 2 * N, *Q3 = a.q + 3 * N, *Q4 = a.q + 4 * N;
   HaloSet<R> hs;
   hs.init(ox, oy, i0, j0, tid, n1);
+  // closure: weights staged once per block, TMEM for the three products (128 lanes x 128 columns)
+  ClSmem *cs = nullptr;
+  __nv_bfloat16 *clX = nullptr, *clH = nullptr;
+  uint32_t cl_phase = 0;
+  int cl_ok = 1;
+  if constexpr (CL) {
+    cs = reinterpret_cast<ClSmem *>(smem_raw + cl_offset_g<T, R>());
+    unsigned char *act = cl_alias_plane<T, R>() ? smem_raw : smem_raw + cl_offset_g<T, R>() + ((sizeof(ClSmem) + 1023) / 1024) * 1024;
+    clX = reinterpret_cast<__nv_bfloat16 *>(act);
+    clH = clX + 128 * 16;
+    mlp::stage_weights(a.cl_P, cs->W1, cs->W2, cs->W3, nullptr, nullptr);
+    if (tid < mlp::HID) {
+      cs->b1[tid] = a.cl_P[mlp::OB1 + tid];
+      cs->b2[tid] = a.cl_P[mlp::OB2 + tid];
+    }
+    if (tid < 16) cs->b3[tid] = tid < mlp::OUT ? a.cl_P[mlp::OB3 + tid] : 0.0f;
+    if (tid == 0) tc::mbar_init(&cs->mbar, 1);
+    if (ty == 0) tc::tmem_alloc(&cs->tmem, 128);
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+  }
 
   auto put_ring = [&](int kk, double r, double ru, double rv, double rw, double p) {
     const int sl = ((kk % NS) + NS) % NS;
@@ -106,6 +151,8 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_pass_g(const
   halo_fetch(k0);
 
   for (int k = k0; k < k1; ++k) {
+    T outv[CL ? NG : 1];                               // closure: pass-G outputs held across the network
+    float feat[CL ? mlp::IN : 1];
     if (pf_ok) put_ring(k + R, pf[0], pf[1], pf[2], pf[3], pf[4]);
     const int slot = k % NS;
     {
@@ -202,25 +249,108 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_pass_g(const
       const T c4 = -a3x - a3y - a3z - pz;
       T c5 = T(gt) * (-ex - ey - ez);
       c5 = c5 + uc * px + vc * py + wc * pz;
-      T *go = static_cast<T *>(a.gbuf);
-      const long long pt = i + (long long)n1 * j + kofs;
-      go[pt + 0 * N] = c1;
-      go[pt + 1 * N] = c2;
-      go[pt + 2 * N] = c3;
-      go[pt + 3 * N] = c4;
-      go[pt + 4 * N] = c5;
-      go[pt + 5 * N] = t11;
-      go[pt + 6 * N] = t12;
-      go[pt + 7 * N] = t13;
-      go[pt + 8 * N] = t22;
-      go[pt + 9 * N] = t23;
-      go[pt + 10 * N] = t33;
-      go[pt + 11 * N] = lam * tgx;
-      go[pt + 12 * N] = lam * tgy;
-      go[pt + 13 * N] = lam * tgz;
-      go[pt + 14 * N] = phi;
+      const T o[NG] = {c1, c2, c3, c4, c5, t11, t12, t13, t22, t23, t33, lam * tgx, lam * tgy, lam * tgz, phi};
+      if constexpr (CL) {
+#pragma unroll
+        for (int f = 0; f < NG; ++f) outv[f] = o[f];
+        // features of the closure (the unfused path's order): grad u, rho, T, filter width; or the
+        // scale-free form grad u / g, rho, T, g delta with g = |grad u|
+        const double gr[9] = {double(ux), double(uy), double(uz), double(vx), double(vy), double(vz),
+                              double(wx), double(wy), double(wz)};
+        double g2 = 0.0;
+#pragma unroll
+        for (int f = 0; f < 9; ++f) g2 += gr[f] * gr[f];
+        const double gm = sqrt(g2), ginv = gm > 0.0 ? 1.0 / gm : 0.0;
+#pragma unroll
+        for (int f = 0; f < 9; ++f) feat[f] = (float)(a.cl_norm ? gr[f] * ginv : gr[f]);
+        feat[9] = (float)a.q[i + (long long)n1 * j + kofs];
+        feat[10] = (float)Tabs;
+        feat[11] = (float)(a.cl_norm ? gm * a.cl_delta : a.cl_delta);
+      } else {
+        T *go = static_cast<T *>(a.gbuf);
+        const long long pt = i + (long long)n1 * j + kofs;
+#pragma unroll
+        for (int f = 0; f < NG; ++f) go[pt + f * N] = o[f];
+      }
+    }
+    if constexpr (CL) {
+      // the network on the block's 128 points: thread = point = TMEM lane (tcgen05, BF16 operands)
+      __syncthreads();                             // every plane read done: X / H may reuse the plane
+      float v[16];
+#pragma unroll
+      for (int f = 0; f < 16; ++f) v[f] = 0.0f;
+      if (inside) {
+#pragma unroll
+        for (int f = 0; f < mlp::IN; ++f) v[f] = (feat[f] - a.cl_sc.in_mean[f]) * a.cl_sc.in_inv[f];
+      }
+      mlp::put8(clX, tid, 0, 16, v);
+      mlp::put8(clX, tid, 8, 16, v + 8);
+      const uint32_t tb = cs->tmem, lane = (uint32_t)(ty * 32) << 16;
+      auto mma = [&](uint32_t col, const __nv_bfloat16 *A, const __nv_bfloat16 *B, int K, int Nn) {
+        tc::fence_before();
+        tc::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+          tc::fence_after();
+          tc::gemm_bf16(tb + col, tc::smem_addr(A), tc::smem_addr(B), K, Nn, false);
+          tc::commit(&cs->mbar);
+        }
+        cl_ok = __syncthreads_and(cl_ok && tc::mbar_wait(&cs->mbar, cl_phase, mlp::kWaitLimit));
+        cl_phase ^= 1;
+        tc::fence_after();
+      };
+      mma(0, clX, cs->W1, 16, 64);
+      for (int c = 0; c < 4 && cl_ok; ++c) {
+        tc::tmem_ld16(tb + lane + c * 16, v);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) v[e] = mlp::gelu(v[e] + cs->b1[c * 16 + e]);
+        mlp::put8(clH, tid, c * 16, 64, v);
+        mlp::put8(clH, tid, c * 16 + 8, 64, v + 8);
+      }
+      if (cl_ok) mma(64, clH, cs->W2, 64, 64);
+      if (cl_ok) {
+        // H1 has been consumed by the finished product: H2 takes its place
+        for (int c = 0; c < 4; ++c) {
+          tc::tmem_ld16(tb + lane + 64 + c * 16, v);
+#pragma unroll
+          for (int e = 0; e < 16; ++e) v[e] = mlp::gelu(v[e] + cs->b2[c * 16 + e]);
+          mlp::put8(clH, tid, c * 16, 64, v);
+          mlp::put8(clH, tid, c * 16 + 8, 64, v + 8);
+        }
+        mma(0, clH, cs->W3, 64, 16);
+      }
+      if (cl_ok) tc::tmem_ld16(tb + lane + 0, v);
+      if (inside && cl_ok) {
+        // model stresses (order 11, 22, 33, 12, 13, 23) in the momentum fluxes: tau_ij - tau_ij(model)
+        const double gd = (double)feat[11];
+        const double scl = a.cl_norm ? (double)feat[9] * gd * gd : 1.0;
+        double tm[mlp::OUT];
+#pragma unroll
+        for (int o2 = 0; o2 < mlp::OUT; ++o2) tm[o2] = (double)((v[o2] + cs->b3[o2]) * a.cl_sc.out_scale[o2]) * scl;
+        outv[5] = T(double(outv[5]) - tm[0]);    // t11
+        outv[6] = T(double(outv[6]) - tm[3]);    // t12
+        outv[7] = T(double(outv[7]) - tm[4]);    // t13
+        outv[8] = T(double(outv[8]) - tm[1]);    // t22
+        outv[9] = T(double(outv[9]) - tm[5]);    // t23
+        outv[10] = T(double(outv[10]) - tm[2]);  // t33
+        T *go = static_cast<T *>(a.gbuf);
+        const long long pt = (i0 + tx) + (long long)n1 * (j0 + ty) + kofs;
+#pragma unroll
+        for (int f = 0; f < NG; ++f) go[pt + f * N] = outv[f];
+      }
+      if (!cl_ok) break;
     }
     __syncthreads();
+  }
+  if constexpr (CL) {
+    if (!cl_ok) {
+      if (tid == 0) atomicExch(a.cl_err, 1);
+      tc::mbar_wait(&cs->mbar, cl_phase, mlp::kWaitLimit);   // a product still in flight ends first
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (ty == 0) tc::tmem_free(cs->tmem, 128);
   }
 }
 
@@ -233,7 +363,7 @@ __global__ void __launch_bounds__(TX *TY, 3) k_pass_d(const __grid_constant__ Fu
   constexpr int PW = TX + 2 * R, PH = TY + 2 * R, PS = PW * PH;
   constexpr int NS = ring_slots(R);
   constexpr int NRF = 4, RS = TX * TY;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   T *plane = reinterpret_cast<T *>(smem_raw);          // [7][PH][PW]
   T *ring = plane + 7 * PS;                            // [NS][NRF][TY*TX]
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -415,6 +545,10 @@ size_t smem_g() {
   return sizeof(T) * (7 * (TX + 2 * R) * (TY + 2 * R) + ring_slots(R) * 6 * TX * TY);
 }
 template <typename T, int R>
+size_t smem_g_cl() {
+  return cl_offset_g<T, R>() + ((sizeof(ClSmem) + 1023) / 1024) * 1024 + (cl_alias_plane<T, R>() ? 0 : kClActBytes);
+}
+template <typename T, int R>
 size_t smem_d() {
   return sizeof(T) * (7 * (TX + 2 * R) * (TY + 2 * R) + ring_slots(R) * 4 * TX * TY);
 }
@@ -434,7 +568,19 @@ void launch_passes(cruna_ctx *c, FusedArgs &a) {
   static const int res_d = resident_blocks(k_pass_d<T, R, PER>, TX * TY, smem_d<T, R>());
   const int sms = device_sms();
   int nz = 1;
-  {
+  if (a.cl_P) {                                    // pass G with the closure network in place
+    static bool cl_configured = false;
+    if (!cl_configured) {
+      CRUNA_CUDA_CHECK(cudaFuncSetAttribute(k_pass_g<T, R, PER, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem_g_cl<T, R>()));
+      cl_configured = true;
+    }
+    static const int res_cl = resident_blocks(k_pass_g<T, R, PER, true>, TX * TY, smem_g_cl<T, R>());
+    a.kc = z_chunk_balanced(c->g.n3, bx * by, res_cl, sms, R, nz);
+    ProfScope ps(c, "pass_g_closure");
+    k_pass_g<T, R, PER, true><<<dim3(bx, by, nz), dim3(TX, TY), smem_g_cl<T, R>(), c->stream>>>(a);
+    CRUNA_LAUNCH_CHECK(c);
+  } else {
     a.kc = z_chunk_balanced(c->g.n3, bx * by, res_g, sms, R, nz);
     ProfScope ps(c, "pass_g");
     k_pass_g<T, R, PER><<<dim3(bx, by, nz), dim3(TX, TY), smem_g<T, R>(), c->stream>>>(a);
@@ -484,6 +630,9 @@ int halo_of(const LineOp &op) {
 }
 
 }  // namespace fz
+
+// the closure network runs inside pass G (fused RHS path, closure attached and not switched off)
+bool closure_in_pass(const cruna_ctx *c) { return c->closure_mlp && c->closure_fused && use_fused(c); }
 
 bool fused_supported(const cruna_ctx *c) {
   for (int d = 0; d < 3; ++d) {
@@ -538,6 +687,14 @@ void rhs_direct_fused(cruna_ctx *c, const double *q_in, double *rhs, int stage, 
   a.q = q;
   a.gbuf = c->fz;
   a.force = c->force;
+  if (closure_in_pass(c)) {                        // the closure's stresses enter through pass G
+    int *flag = nullptr;
+    mlp_device_view(c->closure_mlp, &a.cl_P, &a.cl_sc, &flag);
+    a.cl_err = flag;
+    a.cl_delta = c->closure_delta;
+    a.cl_norm = c->closure_norm ? 1 : 0;
+    a.force = c->user_force;
+  }
   a.dt = dt;
   a.q0 = q0;
   a.acc = acc;

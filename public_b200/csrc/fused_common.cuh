@@ -7,6 +7,7 @@
 #include <cmath>
 
 #include "cruna_internal.cuh"
+#include "mlp_common.cuh"
 #include "tcgen05.cuh"
 
 namespace cruna {
@@ -43,6 +44,13 @@ struct FusedArgs {
   const double *q0;
   double *acc;
   double *qnext;
+  // learned closure evaluated inside pass G (its CL instantiation): network parameters and scaling,
+  // filter width, scale-free features / outputs, the network's error flag
+  const float *cl_P = nullptr;
+  mlp::Scaling cl_sc;
+  double cl_delta = 0.0;
+  int cl_norm = 0;
+  int *cl_err = nullptr;
 };
 
 __host__ __device__ constexpr int ring_slots(int R) { return 2 * R + 1; }
