@@ -13,6 +13,7 @@
 
     python -m public_b200.closure_study [--n 256] [--factor 4] [--steps 3000] [--every 10]
         [--samples 2000000] [--train-steps 3000] [--batch 4096] [--lr 1e-3] [--normalised] [--json out.json]
+        [--calibrate 0.8 1.0 1.2] [--separate-closure]
 
 --normalised trains and runs the scale-free closure (``cruna_set_closure_normalisation``): features
 grad u / |grad u| and |grad u| delta, targets tau / (rho (|grad u| delta)^2).
@@ -23,6 +24,10 @@ grad u / |grad u| and |grad u| delta, targets tau / (rho (|grad u| delta)^2).
    perturbation constant over the block -- against the coarse gradients over the same time
    (H / every * 2 coarse steps) of the plain and the closure-augmented coarse solve: cosine
    similarity over the momentum components (the initial velocity) and over the whole state.
+
+5. --calibrate a1 a2 ...: a posteriori, the multiplier of the network's stresses among a1, a2, ... whose
+   coarse run tracks the filtered DNS kinetic energy best over the first half of the snapshots; the
+   whole horizon then judges it.  The closure runs inside the flux pass unless --separate-closure.
 
 Prints one JSON object.  Data are synthetic (seeded spectrum, no dataset).
 """
@@ -75,6 +80,7 @@ def run(args) -> dict:
     ke_dns, t_dns = [], []
     with Cruna(Settings.from_dict(s)) as fine, Cruna(Settings.from_dict(sc)) as coarse:
         coarse.set_closure_normalisation(args.normalised)
+        coarse.set_closure_fused(bool(args.fused_closure))
         # initial filtered state (start of both coarse runs)
         fine.box_filter_dev(r, q.data_ptr(), qc.data_ptr(), tau.data_ptr())
         fine.sync()
@@ -139,12 +145,39 @@ def run(args) -> dict:
 
         ke_plain, ms_plain = coarse_run(False)
         ke_model, ms_model = coarse_run(True)
+        calib = None
+        if args.calibrate:
+            # a posteriori: one multiplier of the network's stresses, fitted by coarse runs to the filtered
+            # DNS kinetic energy over the first half of the snapshots only; the whole horizon then judges it
+            half = max(1, snaps // 2)
+
+            def window_err(ke):
+                return float(np.max(np.abs(ke[:half + 1] - np.array(ke_dns[:half + 1])) / np.array(ke_dns[:half + 1])))
+
+            trials = []
+            for alpha in args.calibrate:
+                mlp.set_scaling(in_mean, in_scale, out_scale * alpha)
+                ke_a, _ = coarse_run(True)
+                trials.append((window_err(ke_a), alpha, ke_a))
+            best = min(trials, key=lambda t: t[0])
+            mlp.set_scaling(in_mean, in_scale, out_scale * best[1])
+            ke_cal, ms_cal = coarse_run(True)
+            calib = {"alphas": [t[1] for t in trials], "window_errors": [t[0] for t in trials], "alpha": best[1],
+                     "window_snapshots": half, "ke_closure": ke_cal.tolist(), "gpu_ms": ms_cal}
+            mlp.set_scaling(in_mean, in_scale, out_scale)
         grad = [gradient_comparison(args, H, fine, coarse, mlp, q0, qc0, delta) for H in args.gradient_steps]
         mlp.close()
     ke_dns = np.array(ke_dns)
 
     def err(ke):
         return float(np.max(np.abs(ke - ke_dns) / ke_dns))
+
+    def err0(ke):      # the same difference measured on the initial energy (error of the decay curve)
+        return float(np.max(np.abs(ke - ke_dns)) / ke_dns[0])
+
+    if calib is not None:
+        calib["ke_max_rel_err"] = err(np.array(calib["ke_closure"]))
+        calib["ke_max_err_of_initial"] = err0(np.array(calib["ke_closure"]))
 
     return {
         "workload": f"isotropic turbulence {nf}^3 -> {nc}^3 (box filter x{r}), Mach_t {args.mach_t}, "
@@ -156,6 +189,8 @@ def run(args) -> dict:
         "explained_variance": ev, "train_seconds": train_s,
         "ke_decay_dns": float(ke_dns[-1] / ke_dns[0]),
         "ke_max_rel_err_plain": err(ke_plain), "ke_max_rel_err_closure": err(ke_model),
+        "ke_max_err_of_initial_plain": err0(ke_plain), "ke_max_err_of_initial_closure": err0(ke_model),
+        "calibration": calib, "closure_in_flux_pass": bool(args.fused_closure),
         "ke_final_rel_err_plain": float(abs(ke_plain[-1] - ke_dns[-1]) / ke_dns[-1]),
         "ke_final_rel_err_closure": float(abs(ke_model[-1] - ke_dns[-1]) / ke_dns[-1]),
         "gpu_ms_dns": dns_ms, "gpu_ms_coarse_plain": ms_plain, "gpu_ms_coarse_closure": ms_model,
@@ -228,6 +263,10 @@ def main(argv=None):
     ap.add_argument("--gradient-steps", type=int, nargs="*", default=[],
                     help="horizons (fine steps) of the fine / coarse gradient comparison")
     ap.add_argument("--gradient-snapshots", type=int, default=64)
+    ap.add_argument("--calibrate", type=float, nargs="*", default=[],
+                    help="multipliers of the network's stresses tried a posteriori (first half of the horizon)")
+    ap.add_argument("--separate-closure", dest="fused_closure", action="store_false",
+                    help="closure as separate launches instead of inside the flux pass")
     ap.add_argument("--json", type=str, default=None)
     args = ap.parse_args(argv)
     out = run(args)

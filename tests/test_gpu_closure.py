@@ -108,7 +108,8 @@ def test_small_closure_study_runs_end_to_end(normalised):
     import argparse
     args = argparse.Namespace(
         n=64, factor=4, steps=40, every=10, samples=8192, train_steps=60, batch=512, lr=2e-3, seed=3,
-        mach_t=0.3, re_lambda=60.0, normalised=normalised, json=None, gradient_steps=[20], gradient_snapshots=8)
+        mach_t=0.3, re_lambda=60.0, normalised=normalised, json=None, gradient_steps=[20], gradient_snapshots=8,
+        calibrate=[], fused_closure=True)
     out = closure_study.run(args)
     assert out["samples"] >= 512
     assert out["train_loss_last"] < out["train_loss_first"]
@@ -158,3 +159,20 @@ def test_normalised_closure_features_and_stage():
     for i in range(3):
         div = sum(O.Dx(cfg, j, T[idx[(i, j)]], dx[j]) for j in range(3))
         assert np.max(np.abs(diff[..., 1 + i] + div)) < 1e-9 * np.max(np.abs(div)) + 1e-12, i
+
+
+def test_trained_closure_beats_the_plain_coarse_solve():
+    """The learned part earns its place: on decaying isotropic turbulence (128^3 DNS -> 32^3, 1200 fine
+    steps, 500k training pairs) the closure-augmented coarse solve tracks the filtered DNS kinetic energy
+    clearly better than the plain filter-stabilised coarse solve (max relative error over the snapshots;
+    measured 12.5 % against 23.8 %)."""
+    from public_b200 import closure_study
+    import argparse
+    args = argparse.Namespace(
+        n=128, factor=4, steps=1200, every=10, samples=500000, train_steps=1500, batch=2048, lr=1e-3, seed=3,
+        mach_t=0.3, re_lambda=100.0, normalised=False, json=None, gradient_steps=[], gradient_snapshots=8,
+        calibrate=[], fused_closure=True)
+    out = closure_study.run(args)
+    assert out["closure_in_flux_pass"]
+    assert out["ke_max_rel_err_closure"] < 0.8 * out["ke_max_rel_err_plain"], (
+        out["ke_max_rel_err_closure"], out["ke_max_rel_err_plain"])
