@@ -14,7 +14,10 @@ point changes branch; the study reports the comparison at two steps (``--eps``, 
 1e-7).
 
     python -m public_b200.gradient_study [--n 128 96 64] [--steps 200] [--nsnap 64] [--ndir 16]
-        [--eps 1e-6 1e-7] [--json out.json]
+        [--eps 1e-6 1e-7] [--fd-dirs K] [--modes 0 1] [--fd-from earlier.json] [--json out.json]
+
+A long horizon can be split over several processes: a run with ``--modes`` (none) computes and stores the
+difference quotients, a later one with ``--fd-from`` reuses them and runs the adjoints.
 """
 from __future__ import annotations
 
@@ -60,9 +63,20 @@ def run(args) -> dict:
         out["J"] = J0
         fd = {}
         t0 = time.time()
+        prior = {}
+        if args.fd_from:
+            # difference quotients of an earlier run of the same workload (same seeded directions)
+            with open(args.fd_from) as fh:
+                old = json.loads(fh.readline())
+            if old.get("workload") != out["workload"]:
+                raise ValueError("--fd-from holds another workload")
+            prior = {float(k): np.array(v) for k, v in old["fd"].items()}
         for eps in args.eps:
+            if eps in prior:
+                fd[eps] = prior[eps]
+                continue
             vals = []
-            for d in dirs:
+            for d in dirs[:args.fd_dirs]:
                 fp = f + eps * d
                 torch.cuda.current_stream().synchronize()
                 c.set_forcing_dev(fp.data_ptr())
@@ -74,8 +88,9 @@ def run(args) -> dict:
                 vals.append((Jp - Jm) / (2 * eps))
             fd[eps] = np.array(vals)
         out["fd_seconds"] = time.time() - t0
+        out["fd"] = {f"{eps:g}": v.tolist() for eps, v in fd.items()}
         c.set_forcing_dev(f.data_ptr())
-        for mode in (0, 1):
+        for mode in args.modes:
             c.set_adjoint_mode(mode)
             torch.cuda.synchronize()
             t0 = time.time()
@@ -83,10 +98,12 @@ def run(args) -> dict:
             c.sync()
             secs = time.time() - t0
             g5 = gf.view(5, N)[4]
-            ad = np.array([float((g5 * d.view(5, N)[4]).sum().item()) for d in dirs])
+            ad_all = np.array([float((g5 * d.view(5, N)[4]).sum().item()) for d in dirs])
             key = "continuous" if mode == 0 else "discrete"
             res = {"J": J, "direct_steps": adv, "seconds": secs}
+            res["directional_derivatives"] = ad_all.tolist()
             for eps, v in fd.items():
+                ad = ad_all[:len(v)]
                 rel = np.abs(ad - v) / np.maximum(np.abs(v), 1e-300)
                 res[f"fd_rel_err_eps{eps:g}"] = {"median": float(np.median(rel)), "max": float(np.max(rel))}
                 res[f"cosine_eps{eps:g}"] = float(np.dot(ad, v) / (np.linalg.norm(ad) * np.linalg.norm(v)))
@@ -103,8 +120,16 @@ def main(argv=None):
     ap.add_argument("--ndir", type=int, default=16)
     ap.add_argument("--y-plane", type=float, default=25.0)
     ap.add_argument("--eps", type=float, nargs="+", default=[1e-6, 1e-7])
+    ap.add_argument("--fd-dirs", type=int, default=None,
+                    help="finite differences on the first K of the ndir directions only (default: all)")
+    ap.add_argument("--fd-from", type=str, default=None,
+                    help="reuse the difference quotients of an earlier run's JSON (same workload)")
+    ap.add_argument("--modes", type=int, nargs="*", default=[0, 1],
+                    help="adjoint modes to run: 0 continuous (reference), 1 exact discrete; none = FD only")
     ap.add_argument("--json", type=str, default=None)
     args = ap.parse_args(argv)
+    if args.fd_dirs is None:
+        args.fd_dirs = args.ndir
     res = run(args)
     line = json.dumps(res)
     print(line)

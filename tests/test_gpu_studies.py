@@ -44,3 +44,20 @@ def test_mlp_bench_small():
     out = mlp_bench.run(argparse.Namespace(n=131072, train_n=16384, batch=1024, steps=5))
     for key in ("forward", "gradient", "train_step"):
         assert np.isfinite(out[key]["ms"]) and out[key]["ms"] > 0
+
+
+def test_gradient_study_split_over_two_runs(tmp_path):
+    """The mixing-layer gradient study split as a long horizon would be: difference quotients first
+    (no adjoint), then both adjoints against the stored quotients; the discrete adjoint matches them."""
+    import json
+
+    from public_b200 import gradient_study
+    base = dict(n=[16, 14, 12], steps=6, nsnap=3, ndir=3, y_plane=25.0, eps=[1e-7], fd_dirs=2)
+    first = gradient_study.run(argparse.Namespace(**base, fd_from=None, modes=[], json=None))
+    assert "continuous" not in first and len(first["fd"]["1e-07"]) == 2
+    path = tmp_path / "fd.json"
+    path.write_text(json.dumps(first) + "\n")
+    second = gradient_study.run(argparse.Namespace(**base, fd_from=str(path), modes=[0, 1], json=None))
+    assert second["fd"] == first["fd"]
+    assert len(second["discrete"]["directional_derivatives"]) == 3
+    assert second["discrete"]["fd_rel_err_eps1e-07"]["max"] < 1e-4
