@@ -212,3 +212,24 @@ def test_continuous_adjoint_is_not_the_discrete_transpose():
         Ldq = (S.rhs_direct(q + eps * dq) - S.rhs_direct(q - eps * dq)) / (2 * eps)
         ratios.append(float(np.sum(S.rhs_adjoint(qs, q, np.zeros_like(q)) * dq)) / float(np.sum(qs * Ldq)))
     assert any(abs(abs(r) - 1.0) > 0.2 for r in ratios), ratios
+
+
+def test_cpu_twin_matches_oracle_mixing_layer():
+    """The C restatement on the mixing-layer scheme set (o6 compact open y-derivatives with dgttrs on the
+    LAPACK factors, the o10 compact open y filter, type-201 characteristic rows at both y ends, the
+    20-point type-400 sponge) reproduces the numpy oracle over 3 direct + adjoint step pairs."""
+    from oracle import cpu_twin
+    n = (24, 20, 16)
+    s, q0 = cases.mixing_layer(n=n)
+    assert cpu_twin.supports(s)
+    fields = {f.name for f in O.dataclasses.fields(O.Config)}
+    S = O.Solver(O.Config(**{k: v for k, v in s.items() if k in fields}), qref=q0.copy())
+    qs0 = cases.smooth_random_state(n, seed=3, p0=0.0, rho0=0.0, amp=1e-2)
+    q, qs = q0.copy(order="F"), qs0.copy(order="F")
+    for it in range(3):
+        q = S.calc_direct(q, 1, nt0=it)
+        qs, _ = S.calc_adjoint(qs, [q, q])
+    qc, qsc = q0.copy(order="F"), qs0.copy(order="F")
+    cpu_twin.run(s, qc, qsc, 3, 2, qref=q0)
+    assert max(O.rel_l2(qc[..., v], q[..., v]) for v in range(5)) < 1e-12
+    assert max(O.rel_l2(qsc[..., v], qs[..., v]) for v in range(5)) < 1e-12
