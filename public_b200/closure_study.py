@@ -25,6 +25,9 @@ grad u / |grad u| and |grad u| delta, targets tau / (rho (|grad u| delta)^2).
    (H / every * 2 coarse steps) of the plain and the closure-augmented coarse solve: cosine
    similarity over the momentum components (the initial velocity) and over the whole state.
 
+--case tgv runs the same pipeline on the Taylor-Green vortex (--mach, --reynolds; the 768^3 -> 192^3
+configuration with --n 768 --precision fp32 for the fine DNS).
+
 5. --calibrate a1 a2 ...: a posteriori, the multiplier of the network's stresses among a1, a2, ... whose
    coarse run tracks the filtered DNS kinetic energy best over the first half of the snapshots; the
    whole horizon then judges it.  The closure runs inside the flux pass unless --separate-closure.
@@ -55,7 +58,10 @@ def run(args) -> dict:
     from .cruna import Cruna, Settings
 
     dev = torch.device("cuda", 0)
-    s, q0 = cases.isotropic_turbulence(n=args.n, seed=args.seed, mach_t=args.mach_t, re_lambda=args.re_lambda)
+    if getattr(args, "case", "isotropic") == "tgv":
+        s, q0 = cases.taylor_green(n=args.n, mach=args.mach, reynolds=args.reynolds, seed=args.seed)
+    else:
+        s, q0 = cases.isotropic_turbulence(n=args.n, seed=args.seed, mach_t=args.mach_t, re_lambda=args.re_lambda)
     nf, r = args.n, args.factor
     nc = nf // r
     dt_f = s["dt"]
@@ -78,7 +84,9 @@ def run(args) -> dict:
     feat = torch.empty((Nc, 12), dtype=torch.float32, device=dev)
     Xs, Ys = [], []
     ke_dns, t_dns = [], []
-    with Cruna(Settings.from_dict(s)) as fine, Cruna(Settings.from_dict(sc)) as coarse:
+    st_fine = Settings.from_dict(s)
+    st_fine.precision = getattr(args, "precision", "fp64")
+    with Cruna(st_fine) as fine, Cruna(Settings.from_dict(sc)) as coarse:
         coarse.set_closure_normalisation(args.normalised)
         coarse.set_closure_fused(bool(args.fused_closure))
         # initial filtered state (start of both coarse runs)
@@ -179,9 +187,14 @@ def run(args) -> dict:
         calib["ke_max_rel_err"] = err(np.array(calib["ke_closure"]))
         calib["ke_max_err_of_initial"] = err0(np.array(calib["ke_closure"]))
 
+    if getattr(args, "case", "isotropic") == "tgv":
+        workload = (f"Taylor-Green {nf}^3 -> {nc}^3 (box filter x{r}), Mach {args.mach}, Re {args.reynolds}, "
+                    f"{args.steps} fine steps, fine DNS in {getattr(args, 'precision', 'fp64')}")
+    else:
+        workload = (f"isotropic turbulence {nf}^3 -> {nc}^3 (box filter x{r}), Mach_t {args.mach_t}, "
+                    f"Re_lambda {args.re_lambda}, {args.steps} fine steps")
     return {
-        "workload": f"isotropic turbulence {nf}^3 -> {nc}^3 (box filter x{r}), Mach_t {args.mach_t}, "
-                    f"Re_lambda {args.re_lambda}, {args.steps} fine steps",
+        "workload": workload,
         "samples": int(X.shape[0]), "train_steps": args.train_steps, "batch": args.batch,
         "normalised": bool(args.normalised),
         "train_loss_first": float(hist[0]) if len(hist) else None,
@@ -263,6 +276,11 @@ def main(argv=None):
     ap.add_argument("--gradient-steps", type=int, nargs="*", default=[],
                     help="horizons (fine steps) of the fine / coarse gradient comparison")
     ap.add_argument("--gradient-snapshots", type=int, default=64)
+    ap.add_argument("--case", default="isotropic", choices=["isotropic", "tgv"],
+                    help="decaying isotropic turbulence (default) or the Taylor-Green vortex")
+    ap.add_argument("--mach", type=float, default=0.2, help="Taylor-Green Mach number")
+    ap.add_argument("--reynolds", type=float, default=3200.0, help="Taylor-Green Reynolds number")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"], help="precision of the fine DNS")
     ap.add_argument("--calibrate", type=float, nargs="*", default=[],
                     help="multipliers of the network's stresses tried a posteriori (first half of the horizon)")
     ap.add_argument("--separate-closure", dest="fused_closure", action="store_false",
