@@ -14,7 +14,8 @@ point changes branch; the study reports the comparison at two steps (``--eps``, 
 1e-7).
 
     python -m public_b200.gradient_study [--n 128 96 64] [--steps 200] [--nsnap 64] [--ndir 16]
-        [--eps 1e-6 1e-7] [--fd-dirs K] [--modes 0 1] [--fd-from earlier.json] [--json out.json]
+        [--eps 1e-6 1e-7] [--fd-dirs K] [--modes 0 1] [--fd-from earlier.json] [--host-snapshots]
+        [--json out.json]
 
 A long horizon can be split over several processes: a run with ``--modes`` (none) computes and stores the
 difference quotients, a later one with ``--fd-from`` reuses them and runs the adjoints.
@@ -90,6 +91,8 @@ def run(args) -> dict:
         out["fd_seconds"] = time.time() - t0
         out["fd"] = {f"{eps:g}": v.tolist() for eps, v in fd.items()}
         c.set_forcing_dev(f.data_ptr())
+        if getattr(args, "host_snapshots", False):
+            c.set_snapshot_memory(True)               # snapshots in pinned host memory, HBM cache of one
         for mode in args.modes:
             c.set_adjoint_mode(mode)
             torch.cuda.synchronize()
@@ -126,6 +129,8 @@ def main(argv=None):
                     help="reuse the difference quotients of an earlier run's JSON (same workload)")
     ap.add_argument("--modes", type=int, nargs="*", default=[0, 1],
                     help="adjoint modes to run: 0 continuous (reference), 1 exact discrete; none = FD only")
+    ap.add_argument("--host-snapshots", action="store_true",
+                    help="keep the binomial snapshots in pinned host memory (states too large for nsnap HBM copies)")
     ap.add_argument("--json", type=str, default=None)
     args = ap.parse_args(argv)
     if args.fd_dirs is None:
