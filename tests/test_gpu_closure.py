@@ -176,3 +176,19 @@ def test_trained_closure_beats_the_plain_coarse_solve():
     assert out["closure_in_flux_pass"]
     assert out["ke_max_rel_err_closure"] < 0.8 * out["ke_max_rel_err_plain"], (
         out["ke_max_rel_err_closure"], out["ke_max_rel_err_plain"])
+
+
+def test_closure_study_on_the_taylor_green_vortex_with_fp32_fine_dns():
+    """The Taylor-Green variant of the closure pipeline (the 768^3 -> 192^3 configuration's code path)
+    on 64^3 -> 16^3 with the fine DNS in FP32 stencils: it trains and both coarse runs stay finite."""
+    from public_b200 import closure_study
+    import argparse
+    args = argparse.Namespace(
+        n=64, factor=4, steps=40, every=10, samples=8192, train_steps=40, batch=512, lr=2e-3, seed=0,
+        mach_t=0.3, re_lambda=60.0, normalised=False, json=None, gradient_steps=[], gradient_snapshots=8,
+        calibrate=[], fused_closure=True, case="tgv", mach=0.2, reynolds=3200.0, precision="fp32")
+    out = closure_study.run(args)
+    assert out["workload"].startswith("Taylor-Green 64^3 -> 16^3") and "fp32" in out["workload"]
+    for key in ("ke_dns", "ke_plain", "ke_closure"):
+        assert len(out[key]) == 5 and all(np.isfinite(out[key]))
+    assert out["train_loss_last"] <= out["train_loss_first"]
