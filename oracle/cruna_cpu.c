@@ -505,10 +505,15 @@ static void filters(const ccpu_cfg *c, double *x, double *buf) {
 }
 
 /* nsteps of (direct step + filters) followed by (adjoint step on the new direct state + filters);
-   qs may be NULL (direct only).  threads <= 0 keeps the OpenMP default.  Returns 0 or -1 (memory). */
+   qs may be NULL (direct only).  threads <= 0 uses the OpenMP default the first call found.  Returns 0 or
+   -1 (memory). */
 int ccpu_run(const ccpu_cfg *c, double *q, double *qs, int nsteps, int threads) {
 #ifdef _OPENMP
-  if (threads > 0) omp_set_num_threads(threads);
+  /* the thread count set here persists in the process: a later call with threads <= 0 returns to the
+     count the first call found */
+  static int default_threads = 0;
+  if (default_threads <= 0) default_threads = omp_get_max_threads();
+  omp_set_num_threads(threads > 0 ? threads : default_threads);
 #else
   (void)threads;
 #endif
