@@ -77,7 +77,7 @@ def run(args) -> dict:
                 fd[eps] = prior[eps]
                 continue
             vals = []
-            for d in dirs[:args.fd_dirs]:
+            for d in dirs[args.fd_start:args.fd_start + args.fd_dirs]:
                 fp = f + eps * d
                 torch.cuda.current_stream().synchronize()
                 c.set_forcing_dev(fp.data_ptr())
@@ -90,6 +90,7 @@ def run(args) -> dict:
             fd[eps] = np.array(vals)
         out["fd_seconds"] = time.time() - t0
         out["fd"] = {f"{eps:g}": v.tolist() for eps, v in fd.items()}
+        out["fd_start"] = args.fd_start
         c.set_forcing_dev(f.data_ptr())
         if getattr(args, "host_snapshots", False):
             c.set_snapshot_memory(True)               # snapshots in pinned host memory, HBM cache of one
@@ -106,7 +107,7 @@ def run(args) -> dict:
             res = {"J": J, "direct_steps": adv, "seconds": secs}
             res["directional_derivatives"] = ad_all.tolist()
             for eps, v in fd.items():
-                ad = ad_all[:len(v)]
+                ad = ad_all[args.fd_start:args.fd_start + len(v)]
                 rel = np.abs(ad - v) / np.maximum(np.abs(v), 1e-300)
                 res[f"fd_rel_err_eps{eps:g}"] = {"median": float(np.median(rel)), "max": float(np.max(rel))}
                 res[f"cosine_eps{eps:g}"] = float(np.dot(ad, v) / (np.linalg.norm(ad) * np.linalg.norm(v)))
@@ -125,6 +126,8 @@ def main(argv=None):
     ap.add_argument("--eps", type=float, nargs="+", default=[1e-6, 1e-7])
     ap.add_argument("--fd-dirs", type=int, default=None,
                     help="finite differences on the first K of the ndir directions only (default: all)")
+    ap.add_argument("--fd-start", type=int, default=0,
+                    help="first of the directions taken by the finite differences (with --fd-dirs: a later slice)")
     ap.add_argument("--fd-from", type=str, default=None,
                     help="reuse the difference quotients of an earlier run's JSON (same workload)")
     ap.add_argument("--modes", type=int, nargs="*", default=[0, 1],

@@ -52,7 +52,7 @@ def test_gradient_study_split_over_two_runs(tmp_path):
     import json
 
     from public_b200 import gradient_study
-    base = dict(n=[16, 14, 12], steps=6, nsnap=3, ndir=3, y_plane=25.0, eps=[1e-7], fd_dirs=2)
+    base = dict(n=[16, 14, 12], steps=6, nsnap=3, ndir=3, y_plane=25.0, eps=[1e-7], fd_dirs=2, fd_start=0)
     first = gradient_study.run(argparse.Namespace(**base, fd_from=None, modes=[], json=None))
     assert "continuous" not in first and len(first["fd"]["1e-07"]) == 2
     path = tmp_path / "fd.json"
