@@ -42,12 +42,17 @@ __device__ __forceinline__ double filt(const FilterArgs &a, const double *p, int
   return p[0] - a.blend * (p[0] - t);
 }
 
-// pass 1: x then y filter of one plane, one variable at a time (tile offsets computed once)
+// pass 1: x then y filter of one plane, one variable at a time (tile offsets computed once).
+// Both directional filters read their taps from per-thread register windows: the x filter takes
+// XQ consecutive points of one row from the tile stored transposed (raw[x][y], consecutive threads on
+// consecutive rows), the y filter RPT consecutive points of one column; the odd row pitches RTS and XFS
+// keep every shared-memory access free of bank conflicts.
 __global__ void __launch_bounds__(FTHR, 4) k_filter_xy(const __grid_constant__ FilterArgs a) {
   constexpr int PW = FXT + 2 * FR, PH = FYT + 2 * FR;
   constexpr int NL = (PW * PH + FTHR - 1) / FTHR;
-  __shared__ double raw[PH * PW];
-  __shared__ double xf[PH * FXT];
+  constexpr int RTS = PH + 1, XFS = FXT + 1;
+  __shared__ double raw[PW * RTS];  // raw[lx * RTS + ly], halo coordinates
+  __shared__ double xf[PH * XFS];   // xf[ly * XFS + x]
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * FXT, j0 = blockIdx.y * FYT, k = blockIdx.z;
   const long long N = a.g.N, n1 = a.g.n1, n12 = (long long)a.g.n1 * a.g.n2;
@@ -71,8 +76,10 @@ __global__ void __launch_bounds__(FTHR, 4) k_filter_xy(const __grid_constant__ F
   for (int v = 0; v < 5; ++v) {
     double *out = a.out + v * N;
 #pragma unroll
-    for (int m = 0; m < NL; ++m)
-      if (goff[m] >= 0) raw[tid + m * FTHR] = nxt[m];
+    for (int m = 0; m < NL; ++m) {
+      const int c = tid + m * FTHR;
+      if (goff[m] >= 0) raw[(c % PW) * RTS + c / PW] = nxt[m];
+    }
     if (v + 1 < 5) {
       const double *in1 = a.in + (v + 1) * N;
 #pragma unroll
@@ -80,10 +87,21 @@ __global__ void __launch_bounds__(FTHR, 4) k_filter_xy(const __grid_constant__ F
         if (goff[m] >= 0) nxt[m] = in1[goff[m] + kofs];
     }
     __syncthreads();
-    for (int c = tid; c < FXT * PH; c += FTHR) {
-      const int lx = c % FXT, ly = c / FXT;
-      const double *p = raw + ly * PW + lx + FR;
-      xf[c] = a.on[0] ? filt(a, p, 1) : p[0];
+    {  // x filter: each thread takes XQ consecutive points of a row (all PH rows, halo rows included)
+      constexpr int XQ = 4, NXW = XQ + 2 * FR;
+      for (int t = tid; t < PH * (FXT / XQ); t += FTHR) {
+        const int ly = t % PH, x0 = (t / PH) * XQ;
+        if (a.on[0]) {
+          double w[NXW];
+#pragma unroll
+          for (int m = 0; m < NXW; ++m) w[m] = raw[(x0 + m) * RTS + ly];
+#pragma unroll
+          for (int u = 0; u < XQ; ++u) xf[ly * XFS + x0 + u] = filt(a, w + u + FR, 1);
+        } else {
+#pragma unroll
+          for (int u = 0; u < XQ; ++u) xf[ly * XFS + x0 + u] = raw[(x0 + u + FR) * RTS + ly];
+        }
+      }
     }
     __syncthreads();
     {  // y filter: each thread takes a column and FYT / 8 consecutive rows from a register window
@@ -91,7 +109,7 @@ __global__ void __launch_bounds__(FTHR, 4) k_filter_xy(const __grid_constant__ F
       const int lx = tid % FXT, ly0 = (tid / FXT) * RPT;
       double w[NW];
 #pragma unroll
-      for (int m = 0; m < NW; ++m) w[m] = xf[(ly0 + m) * FXT + lx];
+      for (int m = 0; m < NW; ++m) w[m] = xf[(ly0 + m) * XFS + lx];
 #pragma unroll
       for (int r = 0; r < RPT; ++r) {
         const int gi = i0 + lx, gj = j0 + ly0 + r;
