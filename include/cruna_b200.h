@@ -39,6 +39,8 @@ extern "C" {
 #define CRUNA_ERR_STATE (-4)     /* non-finite or non-physical state detected (rho <= 0, p <= 0, NaN) */
 #define CRUNA_ERR_UNSUPPORTED (-5) /* boundary type / scheme / path not available */
 #define CRUNA_ERR_NODEVICE (-6)  /* no CUDA device */
+#define CRUNA_ERR_IO (-7)        /* a snapshot / restart file could not be opened, written, renamed or read,
+                                    or is not a file of this library */
 #define CRUNA_STOPPED 1          /* cruna_run_hpc: stopped by its wall-time or step budget after storing
                                     a snapshot and the restart file (not an error) */
 
@@ -394,7 +396,9 @@ int cruna_rhs_direct_noalloc(const cruna_config *cfg, const double *q, double *r
  *   restartfile.bin                                 (the int32 pair (ns, nt) of the last restart point)
  * Layout: 64-byte header (magic "CRUNAB2D", int32 version 1, int32 element size 8 or 4, int64 dims[4],
  * int64 params length, int64 0), the params text ("key = value" lines), the data in Fortran order.
- * Files are written to "<name>.tmp" and renamed.  Context-free functions report errors through
+ * Files are written to "<name>.tmp" and renamed.  A file that cannot be opened, written, renamed or
+ * read, or that is not a file of this library, gives CRUNA_ERR_IO; bad arguments and a shape that differs
+ * from the expected one give CRUNA_ERR_ARG.  Context-free functions report errors through
  * cruna_last_error(NULL).
  */
 /* Writes the file name of `type` ("data_direct_snapshot", "data_adjoint_snapshot", "data_direct",

@@ -42,7 +42,7 @@ ABI_VERSION = 2
 
 CRUNA_STOPPED = 1
 ERRORS = {-1: "CRUNA_ERR_ARG", -2: "CRUNA_ERR_CUDA", -3: "CRUNA_ERR_NOMEM", -4: "CRUNA_ERR_STATE",
-          -5: "CRUNA_ERR_UNSUPPORTED", -6: "CRUNA_ERR_NODEVICE"}
+          -5: "CRUNA_ERR_UNSUPPORTED", -6: "CRUNA_ERR_NODEVICE", -7: "CRUNA_ERR_IO"}
 
 
 class CrunaError(RuntimeError):

@@ -45,9 +45,14 @@ struct FileHeader {
 };
 static_assert(sizeof(FileHeader) == 64, "file header is 64 bytes");
 
-int io_fail(const std::string &msg) {
+int arg_fail(const std::string &msg) {
   cruna::set_global_error(msg);
   return CRUNA_ERR_ARG;
+}
+
+int io_fail(const std::string &msg) {
+  cruna::set_global_error(msg);
+  return CRUNA_ERR_IO;
 }
 
 int write_file(const std::string &path, int elem, const int64_t dims[4], const void *data, const std::string &params) {
@@ -57,7 +62,7 @@ int write_file(const std::string &path, int elem, const int64_t dims[4], const v
   h.elem = elem;
   int64_t count = 1;
   for (int d = 0; d < 4; ++d) {
-    if (dims[d] < 1) return io_fail("snapshot dims must be >= 1");
+    if (dims[d] < 1) return arg_fail("snapshot dims must be >= 1");
     h.dims[d] = dims[d];
     count *= dims[d];
   }
@@ -114,7 +119,7 @@ std::string fmt_int(int v, int width) {
 // io_helper.f90:11-15 formats and the name assembly of :426-432 for the types this library writes
 int make_fname(std::string &out, const char *workdir, const char *type, int world_block, int block_image, int ns,
                int nt) {
-  if (!type) return io_fail("null file type");
+  if (!type) return arg_fail("null file type");
   const std::string wdir = std::string(workdir && *workdir ? workdir : ".") + "/";
   const std::string t(type);
   const std::string blk = "_" + fmt_int(world_block, 2), img = "_" + fmt_int(block_image, 5);
@@ -125,7 +130,7 @@ int make_fname(std::string &out, const char *workdir, const char *type, int worl
   else if (t == "restartfile")                                              // :337-342
     out = wdir + "restartfile";
   else
-    return io_fail("unknown file type " + t);
+    return arg_fail("unknown file type " + t);
   return CRUNA_OK;
 }
 
@@ -164,12 +169,12 @@ int cruna_io_fname(char *buf, int buflen, const char *workdir, const char *type,
 }
 
 int cruna_write_snapshot(const char *path, const int64_t dims[4], const double *data, const char *params) {
-  if (!path || !dims || !data) return io_fail("null argument");
+  if (!path || !dims || !data) return arg_fail("null argument");
   return write_file(path, 8, dims, data, params ? params : "");
 }
 
 int cruna_read_snapshot(const char *path, int64_t dims[4], double *data, char *params, int params_len) {
-  if (!path || !dims) return io_fail("null argument");
+  if (!path || !dims) return arg_fail("null argument");
   FileHeader h;
   std::string txt;
   FILE *f = nullptr;
@@ -179,7 +184,7 @@ int cruna_read_snapshot(const char *path, int64_t dims[4], double *data, char *p
   for (int d = 0; d < 4; ++d) {
     if (data && dims[d] != h.dims[d]) {
       std::fclose(f);
-      return io_fail(std::string(path) + ": shape differs from the expected one");
+      return arg_fail(std::string(path) + ": shape differs from the expected one");
     }
     dims[d] = h.dims[d];
     count *= h.dims[d];
@@ -207,7 +212,7 @@ int cruna_write_restart(const char *workdir, int ns, int nt) {
 }
 
 int cruna_read_restart(const char *workdir, int *ns, int *nt) {
-  if (!ns || !nt) return io_fail("null argument");
+  if (!ns || !nt) return arg_fail("null argument");
   std::string name;
   int rc = make_fname(name, workdir, "restartfile", 1, 1, 0, 0);
   if (rc) return rc;
@@ -230,7 +235,7 @@ int cruna_read_restart(const char *workdir, int *ns, int *nt) {
 }
 
 int cruna_restart_start(int ns, int nt, int steps, int *s0, int *nt0) {
-  if (!s0 || !nt0 || steps < 1) return io_fail("bad arguments to cruna_restart_start");
+  if (!s0 || !nt0 || steps < 1) return arg_fail("bad arguments to cruna_restart_start");
   const long long total = (long long)(ns - 1) * steps + nt + 1;      // cruna_hpc.f90:143-145
   *s0 = (int)(total / steps + 1);
   *nt0 = (int)(total - (long long)(*s0 - 1) * steps);
@@ -238,7 +243,7 @@ int cruna_restart_start(int ns, int nt, int steps, int *s0, int *nt0) {
 }
 
 int cruna_store_snapshot(cruna_ctx *ctx, const char *workdir, const char *type, const double *q, int ns, int nt) {
-  if (!ctx || !q) return io_fail("null argument");
+  if (!ctx || !q) return arg_fail("null argument");
   const cruna_config &c = ctx->cfg;
   std::string name;
   int rc = make_fname(name, workdir, type, 1, 1, ns, nt);
@@ -248,7 +253,7 @@ int cruna_store_snapshot(cruna_ctx *ctx, const char *workdir, const char *type, 
 }
 
 int cruna_load_snapshot(cruna_ctx *ctx, const char *workdir, const char *type, double *q, int ns, int nt) {
-  if (!ctx || !q) return io_fail("null argument");
+  if (!ctx || !q) return arg_fail("null argument");
   const cruna_config &c = ctx->cfg;
   std::string name;
   int rc = make_fname(name, workdir, type, 1, 1, ns, nt);
@@ -258,8 +263,8 @@ int cruna_load_snapshot(cruna_ctx *ctx, const char *workdir, const char *type, d
 }
 
 int cruna_run_hpc(cruna_ctx *ctx, double *q_io, const cruna_hpc_opts *o, int *ns_out, int *nt_out) {
-  if (!ctx || !q_io || !o) return io_fail("null argument");
-  if (o->steps < 1 || o->subsets < 1) return io_fail("cruna_run_hpc: steps and subsets must be >= 1");
+  if (!ctx || !q_io || !o) return arg_fail("null argument");
+  if (o->steps < 1 || o->subsets < 1) return arg_fail("cruna_run_hpc: steps and subsets must be >= 1");
   const cruna_config &c = ctx->cfg;
   ctx->err.clear();
   const long long M = 5LL * c.n[0] * c.n[1] * c.n[2];

@@ -36,14 +36,32 @@ def test_snapshot_round_trip_is_bit_exact(tmp_path):
 def test_corrupt_or_foreign_files_are_rejected(tmp_path):
     path = tmp_path / "bad.bin"
     path.write_bytes(b"not a snapshot at all, just bytes" * 4)
-    with pytest.raises(cruna.CrunaError):
+    with pytest.raises(cruna.CrunaError) as e:
         cruna.read_snapshot(str(path))
+    assert e.value.code == -7                        # CRUNA_ERR_IO
     good = str(tmp_path / "good.bin")
     cruna.write_snapshot(good, np.ones((4, 4, 4, 5), order="F"))
     raw = open(good, "rb").read()
     open(good, "wb").write(raw[:-8])                 # truncated data
-    with pytest.raises(cruna.CrunaError):
+    with pytest.raises(cruna.CrunaError) as e:
         cruna.read_snapshot(good)
+    assert e.value.code == -7
+
+
+def test_file_system_failures_are_io_errors(tmp_path):
+    missing = str(tmp_path / "no_such_dir")
+    with pytest.raises(cruna.CrunaError) as e:
+        cruna.write_snapshot(missing + "/snap.bin", np.ones((2, 2, 2, 5), order="F"))
+    assert e.value.code == -7                        # the .tmp file cannot be opened
+    with pytest.raises(cruna.CrunaError) as e:
+        cruna.read_snapshot(str(tmp_path / "absent.bin"))
+    assert e.value.code == -7
+    with pytest.raises(cruna.CrunaError) as e:
+        cruna.write_restart(missing, 1, 2)
+    assert e.value.code == -7
+    with pytest.raises(cruna.CrunaError) as e:
+        cruna.io_fname(str(tmp_path), "no_such_type")
+    assert e.value.code == -1                        # an argument error, not I/O
 
 
 def test_restartfile_round_trip_and_absence(tmp_path):
