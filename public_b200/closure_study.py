@@ -30,7 +30,7 @@ configuration with --n 768 --precision fp32 for the fine DNS).
 
 5. --calibrate a1 a2 ...: a posteriori, the multiplier of the network's stresses among a1, a2, ... whose
    coarse run tracks the filtered DNS kinetic energy best over the first half of the snapshots; the
-   whole horizon then judges it.  The closure runs inside the flux pass unless --separate-closure.
+   whole horizon then scores it.  The closure runs inside the flux pass unless --separate-closure.
 
 Prints one JSON object.  Data are synthetic (seeded spectrum, no dataset).
 """
@@ -156,7 +156,7 @@ def run(args) -> dict:
         calib = None
         if args.calibrate:
             # a posteriori: one multiplier of the network's stresses, fitted by coarse runs to the filtered
-            # DNS kinetic energy over the first half of the snapshots only; the whole horizon then judges it
+            # DNS kinetic energy over the first half of the snapshots only; the whole horizon then scores it
             half = max(1, snaps // 2)
 
             def window_err(ke):

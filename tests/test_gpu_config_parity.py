@@ -27,7 +27,7 @@ CFG_FIELDS = {f.name for f in O.dataclasses.fields(O.Config)}
 def rel_l2_state(a, b):
     """Relative L2 per conservative variable; momentum components are measured against
     max(their own norm, |rho| * c), the sound-speed scale, so a component that is small by symmetry
-    is not judged on its own tiny norm."""
+    is not measured against its own tiny norm."""
     rho, p = b[..., 0], b[..., 4]
     c = float(np.sqrt(1.4 * np.mean(np.abs(p)) / np.mean(np.abs(rho))))
     out = []
