@@ -9,6 +9,10 @@ Legs (grid point-steps per second; the state generated once, one untimed warm-up
   tgv      Taylor-Green 256^3, 2 direct + 2 adjoint steps on all threads; 128^3, 1 + 1 on one thread
   mixing   mixing layer 512 x 384 x 256 (o6 compact y, o10 open filter, type-201 rows, sponge),
            3 direct + 3 adjoint steps on all threads
+  closure  the closure configuration's coarse grid: isotropic turbulence 64^3, 100 direct steps of the
+           plain filter-stabilised solve on all threads and 20 on one; the closure network
+           (12 -> 64 -> 64 -> 6, GELU) in FP32 on the host cores through torch, forward and
+           forward + backward of a mean-squared loss on 10^5 samples (best of 3 after a warm-up)
 Direct and adjoint rates are separated by timing direct-only steps, then direct + adjoint pairs.
 """
 from __future__ import annotations
@@ -70,12 +74,52 @@ def run(legs) -> dict:
         s, q0 = cases.mixing_layer(n=(512, 384, 256))
         assert cpu_twin.supports(s)
         res["mixing_layer_512x384x256"] = {"all": _leg(s, q0, q0, 3, 0, True)}
+    if "closure" in legs:
+        s, q0 = cases.isotropic_turbulence(n=64)
+        assert cpu_twin.supports(s)
+        res["isotropic_coarse_64"] = {"all": _leg(s, q0, None, 100, 0, False), "one": _leg(s, q0, None, 20, 1, False)}
+        res["closure_mlp_1e5_samples"] = _mlp_leg(100_000)
     return res
+
+
+def _mlp_leg(n: int) -> dict:
+    """The closure network on the host cores: torch FP32 (its CPU kernels, all its threads), samples/s of
+    the forward pass and of forward + backward of a mean-squared loss."""
+    import torch
+    from oracle import cpu_twin
+
+    torch.set_num_threads(cpu_twin.threads())        # a one-thread leg before may have left the pool at 1
+    torch.manual_seed(0)
+    net = torch.nn.Sequential(torch.nn.Linear(12, 64), torch.nn.GELU(), torch.nn.Linear(64, 64), torch.nn.GELU(),
+                              torch.nn.Linear(64, 6))
+    X = torch.randn(n, 12)
+    Y = torch.randn(n, 6)
+
+    def fwd():
+        with torch.no_grad():
+            net(X)
+
+    def grad():
+        net.zero_grad(set_to_none=True)
+        torch.mean((net(X) - Y) ** 2).backward()
+
+    out = {"samples": n, "threads": torch.get_num_threads(), "dtype": "f32"}
+    for name, fn in (("forward", fwd), ("gradient", grad)):
+        fn()
+        best = float("inf")
+        for _ in range(3):
+            t0 = time.perf_counter()
+            fn()
+            best = min(best, time.perf_counter() - t0)
+        out[f"{name}_seconds"] = best
+        out[f"{name}_samples_per_s"] = n / best
+    return out
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("--legs", nargs="+", default=["vortex", "tgv", "mixing"], choices=["vortex", "tgv", "mixing"])
+    ap.add_argument("--legs", nargs="+", default=["vortex", "tgv", "mixing"],
+                    choices=["vortex", "tgv", "mixing", "closure"])
     ap.add_argument("--json", type=str, default=None)
     args = ap.parse_args(argv)
     out = run(args.legs)

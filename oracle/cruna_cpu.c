@@ -507,13 +507,20 @@ static void filters(const ccpu_cfg *c, double *x, double *buf) {
 /* nsteps of (direct step + filters) followed by (adjoint step on the new direct state + filters);
    qs may be NULL (direct only).  threads <= 0 uses the OpenMP default the first call found.  Returns 0 or
    -1 (memory). */
+#ifdef _OPENMP
+/* the OpenMP thread count of the process before any call here changed it */
+static int default_threads(void) {
+  static int n = 0;
+  if (n <= 0) n = omp_get_max_threads();
+  return n;
+}
+#endif
+
 int ccpu_run(const ccpu_cfg *c, double *q, double *qs, int nsteps, int threads) {
 #ifdef _OPENMP
   /* the thread count set here persists in the process: a later call with threads <= 0 returns to the
      count the first call found */
-  static int default_threads = 0;
-  if (default_threads <= 0) default_threads = omp_get_max_threads();
-  omp_set_num_threads(threads > 0 ? threads : default_threads);
+  omp_set_num_threads(threads > 0 ? threads : default_threads());
 #else
   (void)threads;
 #endif
@@ -535,9 +542,10 @@ int ccpu_run(const ccpu_cfg *c, double *q, double *qs, int nsteps, int threads) 
   return 0;
 }
 
+/* the thread count a call with threads <= 0 uses (the process default, whatever an earlier call set) */
 int ccpu_threads(void) {
 #ifdef _OPENMP
-  return omp_get_max_threads();
+  return default_threads();
 #else
   return 1;
 #endif
